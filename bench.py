@@ -1,0 +1,304 @@
+"""Benchmark of the plain FP64 MHD step (HLLD, minmod, Heun RK2) on a 256^3 Cartesian grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 256]
+                    [--tsteps 200]
+
+One bench step = one solve of the workload: `--tsteps` (200) time steps of the 256^3 grid.
+Prints one JSON line on rank 0.
+
+  value     cell-updates/s over the K timed solves, state resident in HBM (1.07 GB per buffer,
+            far above the 126 MB L2), CUDA events on the solver's stream, max over ranks.
+  e2e       the same metric through the C ABI with host buffers: every step uploads Cell_par
+            (setb_set_state, pinned host memory), runs the solve, downloads Cell_par
+            (setb_get_state); device-timed with events on the solver's stream.
+  roofline  per-kernel CUDA-event times over the timed region (setb_step_profiled); algorithmic
+            bytes per cell-update: 128 B for the first stage (read U^n, write U*), 192 B for the
+            second (read U*, U^n, write U^n+1).
+  cpu_baseline  the CPU oracle (a port of the reference algorithm) on this host's cores, one
+            RK2 step of the same grid.
+N > 1 runs N independent replicas (weak scaling): no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
+BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
+BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        busy = [x for x in sm if smax and x > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(n: int, tsteps_sample: int = 1):
+    """The oracle (CPU port of the reference algorithm) on all host threads: one RK2 HLLD step
+    of the n^3 grid; returns cell-updates/s and the thread count."""
+    import numpy as np  # noqa: F401
+    import oracle as O
+    O.build()
+    g = O.make_grid(n, r_floor=0.5 * 2.0 / n)
+    U = O.init_lism(g, seed=2)
+    ck = O.clock_init(g)
+    ck.dt_next = 1e-4
+    threads = O.max_threads()
+    t0 = time.perf_counter()
+    O.run(g, O.make_opts(3, 2, 2, 0.4), U, tsteps_sample, ck, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return n ** 3 * tsteps_sample / dt, threads, dt
+
+
+def run_reference(args, world, rank):
+    """`--impl reference`: the reference algorithm's CPU implementation (the oracle port; the
+    CUDA Fortran reference needs nvfortran, which this image lacks) on this host's cores."""
+    if rank != 0:
+        return
+    import oracle as O
+    O.build()
+    n = args.n
+    g = O.make_grid(n, r_floor=0.5 * 2.0 / n)
+    U = O.init_lism(g, seed=2)
+    ck = O.clock_init(g)
+    ck.dt_next = 1e-4
+    threads = O.max_threads()
+    o = O.make_opts(3, 2, 2, 0.4)
+    for _ in range(args.warmup):
+        O.run(g, o, U, 1, ck, nthreads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.run(g, o, U, 1, ck, nthreads=threads)
+    dt = time.perf_counter() - t0
+    value = n ** 3 * args.steps / dt
+    line = {
+        "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args, reference=True),
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid per bench step (of {args.tsteps} per solve)"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args, reference=False):
+    return {"workload": f"C2 plain FP64: ideal MHD, HLLD + minmod + Heun RK2, {args.n}^3 Cartesian, "
+                        f"{args.tsteps} time steps per bench step",
+            "grid": [args.n] * 3, "time_steps_per_step": args.tsteps, "n_state": 3, "order": 2, "scheme": "rk2",
+            "cfl": 0.4, "precision": "plain-fp64",
+            "l2": "inputs larger than L2 (state 1.07 GB per buffer at 256^3)",
+            "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single"}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import set_b200 as S
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n, T = args.n, args.tsteps
+    desc = S.cart_desc(n)
+    ic = S.lism_ic(seed=2 + rank)
+    opts = S.step_opts(n_state=3, order=2, scheme=2, cfl=0.4)
+    solver = S.Solver(desc, ic=ic)
+    stream = torch.cuda.ExternalStream(solver.stream())
+    cells = n ** 3
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        solver.step(T, opts)
+
+    # ---- device-resident timed region (per-kernel events inside setb_step_profiled)
+    barrier()
+    torch.cuda.synchronize()
+    k_ms = [0.0, 0.0]
+    k_n = [0, 0]
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            _, ms, cnt = solver.step_profiled(T, opts)
+            k_ms = [k_ms[i] + ms[i] for i in range(2)]
+            k_n = [k_n[i] + cnt[i] for i in range(2)]
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms_total = max_over_ranks(ev0.elapsed_time(ev1))
+    clocks = clk.summary()
+    diag = solver.status()
+    value = world * cells * T * args.steps / (ms_total / 1e3)
+
+    hbm, peak_kind = peaks()
+    t1 = k_ms[0] / max(k_n[0], 1)
+    t2 = k_ms[1] / max(k_n[1], 1)
+    ach2 = BYTES_STAGE2 * cells / (t2 / 1e3) / 1e9
+    ach_step = BYTES_STEP * cells / ((t1 + t2) / 1e3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers
+    cp = torch.empty((cells, 16), dtype=torch.float64, pin_memory=True).numpy()
+    cp[:] = 0.0
+    cp_init = S.fill_lism(desc, ic)
+    cp[:, :] = cp_init
+    for _ in range(1):
+        solver.set_state(cp, 0.0)
+        solver.step(T, opts)
+        solver.get_state(cp)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        solver.set_state(cp, 0.0)
+        solver.step(T, opts, wait=False)
+        solver.get_state(cp)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e = world * cells * T * args.steps / (e2e_ms / 1e3)
+    finite = bool(np.isfinite(cp[:, :8]).all())
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, thr, secs = cpu_baseline(n)
+        base = {"value": v, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+                "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid ({secs:.1f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": "cell_updates_per_s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded LISM inflow + solar-wind source sphere (the reference measures no dataset)",
+            "config": config_dict(args),
+            "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": cells * 64,
+                    "d2h_bytes_per_step": cells * 64},
+            "roofline": {"bound": "hbm", "kernel": "stage_fp64_kernel<HLLD,minmod,stage2>",
+                         "achieved": ach2, "peak": hbm, "unit": "GB/s", "frac": ach2 / hbm,
+                         "peak_kind": peak_kind, "traffic": None,
+                         "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
+                         "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2}},
+            "cpu_baseline": base,
+            "clocks": clocks,
+            "gpu_launches": int(sum(k_n)),
+            "diag": {"n_pfloor": diag.n_pfloor, "n_negdens": diag.n_negdens, "finite": finite},
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--tsteps", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

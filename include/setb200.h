@@ -1,0 +1,188 @@
+/*
+ * setb200.h -- C ABI of the B200-native ideal-MHD step (libsetb200.so).
+ *
+ * Drop-in boundary for SergeyMSU/SET's FCMHD solver module.  In the reference the boundary is
+ * a set of Fortran modules: STORAGE (host arrays, SET_Fortran_Cuda_MHD/Storage_module.f90),
+ * MY_CUDA (device arrays, Set_CUDA / CUDA_START_MGD / Send_data_to_Host,
+ * SET_Fortran_Cuda_MHD/cuf_kernel.cuf) and Solvers (chlld, SET_Fortran_Cuda_MHD/Solvers.f90).
+ * Every entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every function returns int32_t status, SETB_OK (0) on success; nothing exits or traps.
+ *   - Host arrays belong to the caller and are copied in and out; device state belongs to the
+ *     handle and stays resident across setb_step calls.
+ *   - Cell_par layout: the reference's Cell_par(16, N), Fortran column-major, i.e. 16 doubles
+ *     per cell, primitive variables (rho, u, v, w, p, Bx, By, Bz, then 8 H-atom fluid values
+ *     that this path carries through untouched).  B is in the reference's stored units: the
+ *     solver uses b = B / sqrt(4*pi).  On a Cartesian grid cell (i, j, k) is column
+ *     1 + i + nx*(j + ny*k).
+ *   - A handle is used by one host thread at a time; each handle owns one CUDA stream.
+ */
+#ifndef SETB200_H
+#define SETB200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SETB_API __attribute__((visibility("default")))
+#else
+#define SETB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define SETB_OK 0
+#define SETB_EINVAL 1     /* bad argument (size, pointer, option)                               */
+#define SETB_ECUDA 2      /* CUDA runtime error                                                 */
+#define SETB_ENOMEM 3     /* device allocation failed or HBM budget exceeded                    */
+#define SETB_ENEGDENS 4   /* a cell update produced rho <= 0 (reference: print + STOP,
+                             cuf_solvers.cuf:708-711); the cell keeps its stage input           */
+#define SETB_EWAVES 5     /* no wave-fan region matched (reference: STOP, Solvers.f90:1816-1825) */
+#define SETB_ERECON 6     /* reconstructed face density < 0 (reference: STOP, cuf_solvers.cuf:414-420) */
+#define SETB_ETIMEOUT 7   /* a bounded device-side wait gave up                                 */
+#define SETB_ENODEV 8     /* no usable CUDA device                                              */
+#define SETB_ESIZE 9      /* size beyond a documented maximum                                   */
+#define SETB_EIO 10       /* file I/O or format/sentinel error                                  */
+#define SETB_EBUSY 11     /* request refused: queue full or admission budget exhausted          */
+
+typedef struct setb_handle setb_handle;
+
+/* ------------------------------------------------------------------ problem description
+ * Uniform Cartesian grid (the reference's face-list geometry with implicit face lists).
+ * Boundaries: ghost cells beyond x = hi[0] hold the fixed `inflow` primitive state; every other
+ * outer boundary is zero-gradient.  Cells whose centre lies at r < r_src from the origin are
+ * re-imposed after every stage with the source state rho = rho_src * (r_src / max(r, r_floor))^2,
+ * radial speed v_src, p = p_over_rho_src * rho, B = 0 (the analogue of the inner boundary of
+ * cuf_solvers.cuf:614-681).  r_src = 0 disables the source. */
+typedef struct {
+    int32_t nx, ny, nz;
+    int32_t flags;          /* reserved, must be 0                                            */
+    double lo[3], hi[3];    /* domain box                                                     */
+    double inflow[8];       /* primitive (rho,u,v,w,p,Bx,By,Bz) beyond x = hi[0]              */
+    double r_src, rho_src, v_src, p_over_rho_src, r_floor;
+    double dt_init;         /* dt of the first step after init / set_state (reference: 2e-9,
+                               cuf_kernel.cuf:758)                                            */
+} setb_cart_desc;
+
+/* Seeded initial condition: uniform LISM state with +-pert_amp relative perturbations of rho and
+ * p drawn by SplitMix64 keyed by (seed, cell index); source state inside r_src. */
+typedef struct {
+    double lism[8];         /* unperturbed primitive state (rho,u,v,w,p,Bx,By,Bz)             */
+    uint64_t seed;
+    double pert_amp;
+} setb_lism_ic;
+
+/* Scheme options (the reference hard-codes them: metod/n_state = 2 at cuf_solvers.cuf:260,
+ * n_disc = 0 at :267, TVD on, RK2 at cuf_kernel.cuf:847-877). */
+typedef struct {
+    int32_t n_state;    /* 3 HLLD, 2 HLLC, 1 HLL, 0 one-speed Lax (chlld n_state)            */
+    int32_t n_disc;     /* chlld n_disc: 0, 1 or 2                                             */
+    int32_t order;      /* 1 first order, 2 minmod reconstruction of rho,u,v,w,p              */
+    int32_t scheme;     /* 1 forward Euler (CUF_MGD_grans/cells), 2 Heun RK2 (CUF_MGD_*_RK2)  */
+    int32_t precision;  /* 0 plain FP64; 1 mixed (FP32 Riemann arithmetic, FP64 state,
+                           compensated update, FP64 pressure recovery and dt)                 */
+    int32_t reserved;   /* must be 0                                                          */
+    double cfl;         /* dt_face = cfl * dist / (max(|SL|,|SR|) + |w|), dist = h/2; the
+                           reference's literal is 0.2 (cuf_solvers.cuf:429)                   */
+} setb_step_opts;
+
+/* Counters and clocks of a handle (replaces the reference's printed diagnostics). */
+typedef struct {
+    double time_all;        /* dev_time_all: simulated time                                   */
+    double dt_next;         /* time_step2: dt the next step will use                          */
+    double dt_last;         /* time_step: dt the last step used                               */
+    int64_t steps;          /* steps taken since init / set_state                             */
+    int64_t n_negdens;      /* cell updates with rho <= 0                                     */
+    int64_t first_bad_cell; /* 0-based cell index of the first such update, -1 if none        */
+    int64_t n_pfloor;       /* pressure floors applied (p <= 0 -> 1e-7, cuf_solvers.cuf:777-779) */
+    int64_t n_wave_err;     /* faces with no matching wave-fan region                         */
+    int64_t n_recon_err;    /* faces with reconstructed rho < 0                               */
+    int64_t n_fp64_redo;    /* mixed form: faces recomputed in FP64 after a positivity failure */
+} setb_diag;
+
+/* ------------------------------------------------------------------ scalar flux routine
+ * Replaces: subroutine chlld(n_state, al, be, ge, w, qqq1, qqq2, dsl, dsp, dsc, qqq, n_disc)
+ *           SET_Fortran_Cuda_MHD/Solvers.f90:1144-1147 (host+device).
+ * Fortran calling convention (all by reference) so a bind(C) interface can call it directly.
+ * n_disc may be NULL (the Fortran OPTIONAL argument, default 0).  Runs on the host. */
+SETB_API int32_t setb_chlld(const int32_t* n_state, const double* al, const double* be, const double* ge,
+                   const double* w, const double qqq1[8], const double qqq2[8], double* dsl,
+                   double* dsp, double* dsc, double qqq[8], const int32_t* n_disc);
+
+/* Batched chlld on the GPU: n independent faces, host arrays, each face k uses normal
+ * normals[3k..3k+2], face speed w[k] (NULL = 0), states q1[8k..], q2[8k..]; writes qqq[8k..],
+ * speeds[3k..] = (dsl, dsp, dsc) and flags[k] (0 ok, 1 wave-fan failure).
+ * precision 0 = FP64 arithmetic, 1 = FP32 arithmetic (the mixed form's solver).
+ * Replaces the per-face chlld call inside CUF_MGD_grans_RK2 (cuf_solvers.cuf:423-426). */
+SETB_API int32_t setb_chlld_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t precision,
+                         const double* normals, const double* w, const double* q1, const double* q2,
+                         double* qqq, double* speeds, int32_t* flags);
+
+/* ------------------------------------------------------------------ device-resident solver
+ * Replaces Set_CUDA (cuf_kernel.cuf:351-382): allocate device state and upload Cell_par. */
+SETB_API int32_t setb_init_cartesian(setb_handle** h, const setb_cart_desc* d, const double* cell_par);
+
+/* As setb_init_cartesian, but the seeded initial condition is generated on the device (no host
+ * Cell_par, no host-to-device copy of the state). */
+SETB_API int32_t setb_init_cartesian_lism(setb_handle** h, const setb_cart_desc* d, const setb_lism_ic* ic);
+
+/* Host-side generator of the same seeded initial condition into a caller Cell_par(16,N);
+ * columns 9..16 are left untouched. */
+SETB_API int32_t setb_cart_fill_lism(const setb_cart_desc* d, const setb_lism_ic* ic, double* cell_par);
+
+/* Replaces one pass of the CUDA_START_MGD time loop (cuf_kernel.cuf:780-925) for nsteps steps:
+ * lagged dt, face fluxes computed once per face, owner-signed conservative update, Euler or
+ * Heun RK2.  Runs asynchronously on the handle's stream when time_all is NULL; otherwise waits
+ * and writes the simulated time.  Device-side errors are reported by setb_step's return value
+ * when it waits, else by the next setb_status / setb_sync. */
+SETB_API int32_t setb_step(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all);
+
+/* As setb_step (always waits), and times every kernel launch with CUDA events recorded on the
+ * handle's stream between consecutive launches: kernel_ms[0] = total ms of the first-stage (or
+ * Euler) kernels, kernel_ms[1] = total ms of the second-stage kernels; launches[0..1] = counts.
+ * Replaces the reference's single event pair around the whole run (cuf_kernel.cuf:760-762,
+ * 930-933). */
+SETB_API int32_t setb_step_profiled(setb_handle* h, int32_t nsteps, const setb_step_opts* o,
+                                    double* time_all, double kernel_ms[2], int32_t launches[2]);
+
+/* Waits for the handle's stream and returns the first device-side error status (or SETB_OK). */
+SETB_API int32_t setb_sync(setb_handle* h);
+
+/* Replaces Send_data_to_Host (cuf_kernel.cuf:384-400): download Cell_par columns 1..8 (columns
+ * 9..16 of the caller's array are left untouched) and the simulated time. */
+SETB_API int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_all);
+
+/* Replaces Fill_data (Storage_module.f90:191-209) as a restart point: upload Cell_par columns
+ * 1..8, set the simulated time, reset the lagged dt to dt_init and clear the counters. */
+SETB_API int32_t setb_set_state(setb_handle* h, const double* cell_par, double time_all);
+
+/* Device pointers of the conserved state (rho, mx, my, mz, E, Bx, By, Bz), structure of arrays:
+ * variable v of cell (i,j,k) is at base[v*var_stride + k*plane_stride + j*row_pitch + i]. */
+SETB_API int32_t setb_state_view(setb_handle* h, double** base, int64_t* var_stride, int64_t* plane_stride,
+                        int64_t* row_pitch);
+
+/* Downloads the conserved state (rho, mx, my, mz, E, Bx, By, Bz) as 8 packed host planes of
+ * N = nx*ny*nz doubles (U[v*N + cell]), the layout the device holds it in. */
+SETB_API int32_t setb_get_conserved(setb_handle* h, double* U);
+
+/* Counters and clocks (replaces the reference's prints). Waits for the handle's stream. */
+SETB_API int32_t setb_status(setb_handle* h, setb_diag* out);
+
+/* The CUDA stream the handle launches on (as a void* cudaStream_t). */
+SETB_API int32_t setb_stream(setb_handle* h, void** stream);
+
+SETB_API int32_t setb_destroy(setb_handle* h);
+
+SETB_API const char* setb_strerror(int32_t code);
+
+/* Library version, e.g. 100 for 1.0.0. */
+SETB_API int32_t setb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SETB200_H */

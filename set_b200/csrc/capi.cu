@@ -1,0 +1,552 @@
+// capi.cu -- host runtime and the C ABI of libsetb200.so (declared in include/setb200.h).
+//
+// The reference drives its kernels from the Fortran module MY_CUDA: Set_CUDA allocates and
+// uploads (cuf_kernel.cuf:351-382), CUDA_START_MGD runs the time loop with 4 launches and 5
+// device-wide synchronisations per step (:780-925), Send_data_to_Host downloads (:384-400).
+// Here a handle owns the device state and one stream; a step is 2 launches (Heun) or 1
+// (Euler) with no host synchronisation, and the lagged dt lives on the device.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "setb200.h"
+#include "setb_internal.cuh"
+
+using namespace sb;
+
+struct setb_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    setb_cart_desc desc{};
+    GridGeom g{};
+    double* buf[2] = {nullptr, nullptr};   // conserved SoA, 8 * vs doubles each
+    int cur = 0;                           // buf[cur] holds U^n
+    DevClock* clk = nullptr;
+    DevStatus* st = nullptr;
+    DevClock* h_clk = nullptr;             // pinned mirrors
+    DevStatus* h_st = nullptr;
+    int ctas_per_sm = 1;
+    int sm_count = 148;
+};
+
+namespace {
+
+#define SB_TRY(expr)                                   \
+    do {                                               \
+        cudaError_t e_ = (expr);                       \
+        if (e_ != cudaSuccess) return SETB_ECUDA;      \
+    } while (0)
+
+int validate_desc(const setb_cart_desc* d) {
+    if (!d) return SETB_EINVAL;
+    if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->flags != 0) return SETB_EINVAL;
+    if ((long long)d->nx * d->ny * d->nz > (1ll << 31)) return SETB_ESIZE;
+    for (int a = 0; a < 3; a++)
+        if (!(d->hi[a] > d->lo[a])) return SETB_EINVAL;
+    if (!(d->inflow[0] > 0.0) || !(d->inflow[4] > 0.0)) return SETB_EINVAL;
+    if (d->r_src < 0.0 || (d->r_src > 0.0 && !(d->rho_src > 0.0))) return SETB_EINVAL;
+    if (!(d->dt_init > 0.0)) return SETB_EINVAL;
+    return SETB_OK;
+}
+
+int validate_opts(const setb_step_opts* o) {
+    if (!o) return SETB_EINVAL;
+    if (o->n_state < 0 || o->n_state > 3) return SETB_EINVAL;
+    if (o->n_disc < 0 || o->n_disc > 2) return SETB_EINVAL;
+    if (o->order != 1 && o->order != 2) return SETB_EINVAL;
+    if (o->scheme != 1 && o->scheme != 2) return SETB_EINVAL;
+    if (o->precision != 0) return SETB_EINVAL;
+    if (o->reserved != 0) return SETB_EINVAL;
+    if (!(o->cfl > 0.0)) return SETB_EINVAL;
+    return SETB_OK;
+}
+
+GridGeom make_geom(const setb_cart_desc* d) {
+    GridGeom g{};
+    g.nx = d->nx;
+    g.ny = d->ny;
+    g.nz = d->nz;
+    g.px = d->nx;
+    g.ps = (long long)d->nx * d->ny;
+    g.vs = g.ps * d->nz;
+    g.vs = (g.vs + 31) / 32 * 32;   // keep every variable plane 256-byte aligned
+    const int n[3] = {d->nx, d->ny, d->nz};
+    for (int a = 0; a < 3; a++) {
+        g.lo[a] = d->lo[a];
+        g.h[a] = (d->hi[a] - d->lo[a]) / n[a];
+        g.inv_dist[a] = 1.0 / (0.5 * g.h[a]);
+    }
+    g.square[0] = g.h[1] * g.h[2];
+    g.square[1] = g.h[0] * g.h[2];
+    g.square[2] = g.h[0] * g.h[1];
+    g.inv_vol = 1.0 / (g.h[0] * g.h[1] * g.h[2]);
+    for (int v = 0; v < 8; v++) g.inflow[v] = d->inflow[v];
+    g.r_src = d->r_src;
+    g.rho_src = d->rho_src;
+    g.v_src = d->v_src;
+    g.p_over_rho_src = d->p_over_rho_src;
+    g.r_floor = d->r_floor;
+    g.lz = d->nz;
+    return g;
+}
+
+// z extent of one CTA's march: balances wave quantisation against the per-chunk prologue
+// (4 plane loads + 1 z face, costed as ~1.5 plane iterations).
+int choose_lz(const GridGeom& g, int sm_count, int ctas_per_sm) {
+    const long long cols = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+    const long long slots = (long long)sm_count * std::max(ctas_per_sm, 1);
+    double best = 1e300;
+    int best_lz = g.nz;
+    for (int c = 1; c <= std::max(1, g.nz / 8); c++) {
+        const int lz = (g.nz + c - 1) / c;
+        const long long ctas = cols * ((g.nz + lz - 1) / lz);
+        const long long waves = (ctas + slots - 1) / slots;
+        const double cost = (double)waves * (lz + 1.5);
+        if (cost < best - 1e-9) {
+            best = cost;
+            best_lz = lz;
+        }
+    }
+    return best_lz;
+}
+
+void clock_reset(setb_handle* h, double time_all) {
+    DevClock c{};
+    c.dt_cur = h->desc.dt_init;
+    c.dt_next = 0;
+    double reset = kDtReset;
+    std::memcpy(&c.dt_next, &reset, sizeof(double));
+    c.time_all = time_all;
+    c.dt_last = 0.0;
+    c.counter = 0;
+    c.steps = 0;
+    *h->h_clk = c;
+    DevStatus s{};
+    s.first_bad = ULLONG_MAX;
+    *h->h_st = s;
+}
+
+int upload_clock(setb_handle* h) {
+    SB_TRY(cudaMemcpyAsync(h->clk, h->h_clk, sizeof(DevClock), cudaMemcpyHostToDevice, h->stream));
+    SB_TRY(cudaMemcpyAsync(h->st, h->h_st, sizeof(DevStatus), cudaMemcpyHostToDevice, h->stream));
+    SB_TRY(cudaStreamSynchronize(h->stream));
+    return SETB_OK;
+}
+
+int download_clock(setb_handle* h) {
+    SB_TRY(cudaMemcpyAsync(h->h_clk, h->clk, sizeof(DevClock), cudaMemcpyDeviceToHost, h->stream));
+    SB_TRY(cudaMemcpyAsync(h->h_st, h->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, h->stream));
+    SB_TRY(cudaStreamSynchronize(h->stream));
+    return SETB_OK;
+}
+
+int status_code(const DevStatus& s) {
+    if (s.n_negdens) return SETB_ENEGDENS;
+    if (s.n_wave) return SETB_EWAVES;
+    if (s.n_recon) return SETB_ERECON;
+    return SETB_OK;
+}
+
+void destroy_impl(setb_handle* h) {
+    if (!h) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (double* b : h->buf)
+        if (b) cudaFree(b);
+    if (h->clk) cudaFree(h->clk);
+    if (h->st) cudaFree(h->st);
+    if (h->h_clk) cudaFreeHost(h->h_clk);
+    if (h->h_st) cudaFreeHost(h->h_st);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaSetDevice(prev);
+    delete h;
+}
+
+int create_impl(setb_handle** out, const setb_cart_desc* d) {
+    if (!out) return SETB_EINVAL;
+    *out = nullptr;
+    int rc = validate_desc(d);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SETB_ENODEV;
+    setb_handle* h = new (std::nothrow) setb_handle();
+    if (!h) return SETB_ENOMEM;
+    cudaGetDevice(&h->device);
+    h->desc = *d;
+    h->g = make_geom(d);
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) {
+        delete h;
+        return SETB_ECUDA;
+    }
+    h->sm_count = prop.multiProcessorCount;
+    h->ctas_per_sm = std::max(1, (int)(prop.sharedMemPerMultiprocessor / (stage_fp64_smem_bytes() + 2048)));
+    h->ctas_per_sm = std::min(h->ctas_per_sm, 1);   // 256 threads x up to 255 registers
+    h->g.lz = choose_lz(h->g, h->sm_count, h->ctas_per_sm);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return SETB_ECUDA;
+    }
+    const size_t bytes = sizeof(double) * 8 * (size_t)h->g.vs;
+    for (int b = 0; b < 2; b++) {
+        if (cudaMalloc(&h->buf[b], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            destroy_impl(h);
+            return SETB_ENOMEM;
+        }
+    }
+    if (cudaMalloc(&h->clk, sizeof(DevClock)) != cudaSuccess || cudaMalloc(&h->st, sizeof(DevStatus)) != cudaSuccess ||
+        cudaMallocHost(&h->h_clk, sizeof(DevClock)) != cudaSuccess ||
+        cudaMallocHost(&h->h_st, sizeof(DevStatus)) != cudaSuccess) {
+        cudaGetLastError();
+        destroy_impl(h);
+        return SETB_ENOMEM;
+    }
+    *out = h;
+    return SETB_OK;
+}
+
+// Uploads Cell_par columns 1..8 (16 doubles per cell) into buf[cur] through buf[1-cur].
+int upload_cellpar(setb_handle* h, const double* cell_par) {
+    const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    double* stage = h->buf[1 - h->cur];
+    SB_TRY(cudaMemcpy2DAsync(stage, 8 * sizeof(double), cell_par, 16 * sizeof(double), 8 * sizeof(double), N,
+                             cudaMemcpyHostToDevice, h->stream));
+    SB_TRY(launch_prim_to_cons(h->g, stage, h->buf[h->cur], h->stream));
+    return SETB_OK;
+}
+
+template <typename T, int NS>
+void chlld_host(const double* n, double w, const double* q1, const double* q2, int n_disc, double* qqq,
+                double* sp, int32_t* fl) {
+    chlld_general<T, NS>(n, w, q1, q2, n_disc, qqq, sp, fl);
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t setb_version(void) { return 100; }
+
+const char* setb_strerror(int32_t code) {
+    switch (code) {
+        case SETB_OK: return "ok";
+        case SETB_EINVAL: return "invalid argument";
+        case SETB_ECUDA: return "CUDA runtime error";
+        case SETB_ENOMEM: return "device allocation failed or memory budget exceeded";
+        case SETB_ENEGDENS: return "cell update produced non-positive density";
+        case SETB_EWAVES: return "no wave-fan region matched in the Riemann solver";
+        case SETB_ERECON: return "reconstructed face density is negative";
+        case SETB_ETIMEOUT: return "bounded device wait gave up";
+        case SETB_ENODEV: return "no usable CUDA device";
+        case SETB_ESIZE: return "size exceeds the documented maximum";
+        case SETB_EIO: return "file I/O or format error";
+        case SETB_EBUSY: return "request refused: queue full or admission budget exhausted";
+        default: return "unknown status code";
+    }
+}
+
+int32_t setb_chlld(const int32_t* n_state, const double* al, const double* be, const double* ge, const double* w,
+                   const double qqq1[8], const double qqq2[8], double* dsl, double* dsp, double* dsc, double qqq[8],
+                   const int32_t* n_disc) {
+    if (!n_state || !al || !be || !ge || !w || !qqq1 || !qqq2 || !dsl || !dsp || !dsc || !qqq) return SETB_EINVAL;
+    const int nd = n_disc ? *n_disc : 0;
+    if (*n_state < 0 || *n_state > 3 || nd < 0 || nd > 2) return SETB_EINVAL;
+    const double n[3] = {*al, *be, *ge};
+    double sp[3];
+    int32_t fl = 0;
+    switch (*n_state) {
+        case 0: chlld_host<double, 0>(n, *w, qqq1, qqq2, nd, qqq, sp, &fl); break;
+        case 1: chlld_host<double, 1>(n, *w, qqq1, qqq2, nd, qqq, sp, &fl); break;
+        case 2: chlld_host<double, 2>(n, *w, qqq1, qqq2, nd, qqq, sp, &fl); break;
+        default: chlld_host<double, 3>(n, *w, qqq1, qqq2, nd, qqq, sp, &fl); break;
+    }
+    *dsl = sp[0];
+    *dsp = sp[1];
+    *dsc = sp[2];
+    return (fl & kFlagWave) ? SETB_EWAVES : SETB_OK;
+}
+
+int32_t setb_chlld_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t precision, const double* normals,
+                         const double* w, const double* q1, const double* q2, double* qqq, double* speeds,
+                         int32_t* flags) {
+    if (n < 0 || n_state < 0 || n_state > 3 || n_disc < 0 || n_disc > 2 || (precision != 0 && precision != 1))
+        return SETB_EINVAL;
+    if (n == 0) return SETB_OK;
+    if (!normals || !q1 || !q2 || !qqq || !speeds || !flags) return SETB_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SETB_ENODEV;
+    double *dn = nullptr, *dw = nullptr, *d1 = nullptr, *d2 = nullptr, *dq = nullptr, *ds = nullptr;
+    int32_t* df = nullptr;
+    cudaStream_t s = nullptr;
+    int rc = SETB_OK;
+    const size_t sn = (size_t)n;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SETB_ECUDA;
+    if (cudaMalloc(&dn, 3 * sn * 8) || (w && cudaMalloc(&dw, sn * 8)) || cudaMalloc(&d1, 8 * sn * 8) ||
+        cudaMalloc(&d2, 8 * sn * 8) || cudaMalloc(&dq, 8 * sn * 8) || cudaMalloc(&ds, 3 * sn * 8) ||
+        cudaMalloc(&df, sn * 4)) {
+        cudaGetLastError();
+        rc = SETB_ENOMEM;
+    }
+    if (rc == SETB_OK) {
+        bool ok = cudaMemcpyAsync(dn, normals, 3 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+                  (!w || cudaMemcpyAsync(dw, w, sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess) &&
+                  cudaMemcpyAsync(d1, q1, 8 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+                  cudaMemcpyAsync(d2, q2, 8 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+                  launch_chlld_batch(n, n_state, n_disc, precision, dn, dw, d1, d2, dq, ds, df, s) == cudaSuccess &&
+                  cudaMemcpyAsync(qqq, dq, 8 * sn * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                  cudaMemcpyAsync(speeds, ds, 3 * sn * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                  cudaMemcpyAsync(flags, df, sn * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                  cudaStreamSynchronize(s) == cudaSuccess;
+        if (!ok) rc = SETB_ECUDA;
+    }
+    cudaFree(dn);
+    cudaFree(dw);
+    cudaFree(d1);
+    cudaFree(d2);
+    cudaFree(dq);
+    cudaFree(ds);
+    cudaFree(df);
+    cudaStreamDestroy(s);
+    return rc;
+}
+
+int32_t setb_cart_fill_lism(const setb_cart_desc* d, const setb_lism_ic* ic, double* cell_par) {
+    int rc = validate_desc(d);
+    if (rc) return rc;
+    if (!ic || !cell_par) return SETB_EINVAL;
+    const GridGeom g = make_geom(d);
+    const long long N = (long long)d->nx * d->ny * d->nz;
+    for (long long c = 0; c < N; c++) {
+        const int i = (int)(c % d->nx);
+        const int j = (int)((c / d->nx) % d->ny);
+        const int k = (int)(c / ((long long)d->nx * d->ny));
+        double q[8];
+        lism_prim(g, ic->lism, ic->seed, ic->pert_amp, i, j, k, q);
+        for (int v = 0; v < 8; v++) cell_par[16 * c + v] = q[v];
+    }
+    return SETB_OK;
+}
+
+int32_t setb_init_cartesian(setb_handle** out, const setb_cart_desc* d, const double* cell_par) {
+    if (!cell_par) return SETB_EINVAL;
+    int rc = create_impl(out, d);
+    if (rc) return rc;
+    setb_handle* h = *out;
+    clock_reset(h, 0.0);
+    rc = upload_cellpar(h, cell_par);
+    if (!rc) rc = upload_clock(h);
+    if (rc) {
+        destroy_impl(h);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int32_t setb_init_cartesian_lism(setb_handle** out, const setb_cart_desc* d, const setb_lism_ic* ic) {
+    if (!ic) return SETB_EINVAL;
+    int rc = create_impl(out, d);
+    if (rc) return rc;
+    setb_handle* h = *out;
+    clock_reset(h, 0.0);
+    double* dl = h->buf[1];   // 8 doubles of scratch for the LISM vector
+    rc = SETB_OK;
+    if (cudaMemcpyAsync(dl, ic->lism, 8 * sizeof(double), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+        launch_lism_init(h->g, dl, ic->seed, ic->pert_amp, h->buf[0], h->stream) != cudaSuccess)
+        rc = SETB_ECUDA;
+    if (!rc) rc = upload_clock(h);
+    if (rc) {
+        destroy_impl(h);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+namespace {
+// Enqueues nsteps steps.  When ev is non-null, ev[0..2*nsteps] are recorded before the first
+// launch and after every launch (Euler: ev[2s+1] == ev[2s+2] bracket nothing).
+int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaEvent_t* ev) {
+    StageArgs a{};
+    a.g = h->g;
+    a.clk = h->clk;
+    a.st = h->st;
+    a.cfl = o->cfl;
+    a.n_disc = o->n_disc;
+    if (ev) SB_TRY(cudaEventRecord(ev[0], h->stream));
+    for (int s = 0; s < nsteps; s++) {
+        double* U = h->buf[h->cur];
+        double* W = h->buf[1 - h->cur];
+        if (o->scheme == 2) {
+            a.Uin = U;
+            a.Ubase = nullptr;
+            a.Uout = W;
+            a.finalize = 0;
+            SB_TRY(launch_stage_fp64(a, o->n_state, o->order, 0, true, h->stream));
+            if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
+            a.Uin = W;
+            a.Ubase = U;
+            a.Uout = U;
+            a.finalize = 1;
+            SB_TRY(launch_stage_fp64(a, o->n_state, o->order, 1, false, h->stream));
+            if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
+        } else {
+            a.Uin = U;
+            a.Ubase = nullptr;
+            a.Uout = W;
+            a.finalize = 1;
+            SB_TRY(launch_stage_fp64(a, o->n_state, o->order, 0, true, h->stream));
+            if (ev) {
+                SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
+                SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
+            }
+            h->cur = 1 - h->cur;
+        }
+    }
+    return SETB_OK;
+}
+}  // namespace
+
+int32_t setb_step(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all) {
+    if (!h || nsteps < 0) return SETB_EINVAL;
+    int rc = validate_opts(o);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    rc = enqueue_steps(h, nsteps, o, nullptr);
+    if (rc) return rc;
+    if (time_all) {
+        rc = download_clock(h);
+        if (rc) return rc;
+        *time_all = h->h_clk->time_all;
+        return status_code(*h->h_st);
+    }
+    return SETB_OK;
+}
+
+int32_t setb_step_profiled(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all,
+                           double kernel_ms[2], int32_t launches[2]) {
+    if (!h || nsteps < 0 || !kernel_ms || !launches) return SETB_EINVAL;
+    int rc = validate_opts(o);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    std::vector<cudaEvent_t> ev(2 * (size_t)nsteps + 1, nullptr);
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            rc = SETB_ECUDA;
+            break;
+        }
+    if (!rc) rc = enqueue_steps(h, nsteps, o, ev.data());
+    kernel_ms[0] = kernel_ms[1] = 0.0;
+    launches[0] = nsteps;
+    launches[1] = o->scheme == 2 ? nsteps : 0;
+    if (!rc && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = SETB_ECUDA;
+    for (int s = 0; s < nsteps && !rc; s++) {
+        float a = 0.f, b = 0.f;
+        if (cudaEventElapsedTime(&a, ev[2 * s], ev[2 * s + 1]) != cudaSuccess ||
+            cudaEventElapsedTime(&b, ev[2 * s + 1], ev[2 * s + 2]) != cudaSuccess) {
+            rc = SETB_ECUDA;
+            break;
+        }
+        kernel_ms[0] += a;
+        kernel_ms[1] += b;
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc) return rc;
+    rc = download_clock(h);
+    if (rc) return rc;
+    if (time_all) *time_all = h->h_clk->time_all;
+    return status_code(*h->h_st);
+}
+
+int32_t setb_sync(setb_handle* h) {
+    if (!h) return SETB_EINVAL;
+    cudaSetDevice(h->device);
+    int rc = download_clock(h);
+    if (rc) return rc;
+    return status_code(*h->h_st);
+}
+
+int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_all) {
+    if (!h || !cell_par) return SETB_EINVAL;
+    cudaSetDevice(h->device);
+    const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    double* stage = h->buf[1 - h->cur];
+    SB_TRY(launch_cons_to_prim(h->g, h->buf[h->cur], stage, h->stream));
+    SB_TRY(cudaMemcpy2DAsync(cell_par, 16 * sizeof(double), stage, 8 * sizeof(double), 8 * sizeof(double), N,
+                             cudaMemcpyDeviceToHost, h->stream));
+    int rc = download_clock(h);
+    if (rc) return rc;
+    if (time_all) *time_all = h->h_clk->time_all;
+    return SETB_OK;
+}
+
+int32_t setb_set_state(setb_handle* h, const double* cell_par, double time_all) {
+    if (!h || !cell_par) return SETB_EINVAL;
+    cudaSetDevice(h->device);
+    SB_TRY(cudaStreamSynchronize(h->stream));
+    clock_reset(h, time_all);
+    int rc = upload_cellpar(h, cell_par);
+    if (rc) return rc;
+    return upload_clock(h);
+}
+
+int32_t setb_state_view(setb_handle* h, double** base, int64_t* var_stride, int64_t* plane_stride,
+                        int64_t* row_pitch) {
+    if (!h) return SETB_EINVAL;
+    if (base) *base = h->buf[h->cur];
+    if (var_stride) *var_stride = h->g.vs;
+    if (plane_stride) *plane_stride = h->g.ps;
+    if (row_pitch) *row_pitch = h->g.px;
+    return SETB_OK;
+}
+
+int32_t setb_get_conserved(setb_handle* h, double* U) {
+    if (!h || !U) return SETB_EINVAL;
+    cudaSetDevice(h->device);
+    const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    for (int v = 0; v < 8; v++)
+        SB_TRY(cudaMemcpyAsync(U + v * N, h->buf[h->cur] + v * h->g.vs, N * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+    SB_TRY(cudaStreamSynchronize(h->stream));
+    return SETB_OK;
+}
+
+int32_t setb_status(setb_handle* h, setb_diag* out) {
+    if (!h || !out) return SETB_EINVAL;
+    cudaSetDevice(h->device);
+    int rc = download_clock(h);
+    if (rc) return rc;
+    const DevClock& c = *h->h_clk;
+    const DevStatus& s = *h->h_st;
+    out->time_all = c.time_all;
+    out->dt_next = c.dt_cur;   // the dt the next step will use
+    out->dt_last = c.dt_last;
+    out->steps = c.steps;
+    out->n_negdens = (int64_t)s.n_negdens;
+    out->first_bad_cell = s.first_bad == ULLONG_MAX ? -1 : (int64_t)s.first_bad;
+    out->n_pfloor = (int64_t)s.n_pfloor;
+    out->n_wave_err = (int64_t)s.n_wave;
+    out->n_recon_err = (int64_t)s.n_recon;
+    out->n_fp64_redo = (int64_t)s.n_redo;
+    return SETB_OK;
+}
+
+int32_t setb_stream(setb_handle* h, void** stream) {
+    if (!h || !stream) return SETB_EINVAL;
+    *stream = (void*)h->stream;
+    return SETB_OK;
+}
+
+int32_t setb_destroy(setb_handle* h) {
+    if (!h) return SETB_EINVAL;
+    destroy_impl(h);
+    return SETB_OK;
+}
+
+}  // extern "C"

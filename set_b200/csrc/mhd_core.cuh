@@ -1,0 +1,414 @@
+// mhd_core.cuh -- the per-face and per-cell arithmetic of the MHD step, written once for the
+// device and the host, templated on the arithmetic type (double for the plain form, float for
+// the Riemann arithmetic of the mixed form).
+//
+// The algorithm is chlld (SET_Fortran_Cuda_MHD/Solvers.f90:1144-1859) with these B200-side
+// design choices, each exact in real arithmetic and differing from the reference only by
+// rounding:
+//   * Faces of the Cartesian grid are axis-aligned, so states arrive already in the face frame
+//     (normal, t1, t2) = a permutation of (x, y, z).  The reference's tangent rotation basis
+//     aco (Solvers.f90:1236-1280) is not built: every chlld formula treats the two tangential
+//     components as a 2-vector (componentwise updates, dot products, sums of squares), so the
+//     flux is the same in any orthonormal tangent basis.
+//   * Divisions by a common denominator become one reciprocal and multiplies; /2 becomes *0.5
+//     (exact); B/sqrt(4*pi) becomes B*(1/sqrt(4*pi)).
+//   * Only the quantities the selected n_state branch reads are formed (e.g. HLLD needs UZ(6)
+//     alone of the HLL average UZ).
+//   * The overlapping "last match wins" IF blocks of the wave-fan selection (:1521-1567,
+//     :1722-1814) are evaluated as the equivalent else-if chain in reverse order.
+#pragma once
+#include <cstdint>
+#include <cmath>
+
+#if defined(__CUDACC__)
+#define SB_HD __host__ __device__ __forceinline__
+#else
+#define SB_HD inline
+#endif
+
+namespace sb {
+
+// Storage_module.f90:8-9 and the derived constants, as correctly rounded doubles.
+constexpr double kCpi4 = 12.566370614359172;        // 4*pi
+constexpr double kSpi4 = 3.5449077018110318;        // sqrt(4*pi)
+constexpr double kInvSpi4 = 0.28209479177387814;    // 1/sqrt(4*pi)
+constexpr double kGamma = 1.6666666666666667;       // 5/3
+constexpr double kG1 = 0.6666666666666667;          // 5/3 - 1
+constexpr double kInvG1 = 1.4999999999999998;       // 1/(5/3 - 1)
+constexpr double kPFloor = 1.0000000116860974e-07;  // FP32 literal 0.0000001 (cuf_solvers.cuf:778)
+constexpr double kDtFaceCap = 100000.0;             // cuf_solvers.cuf:268
+constexpr double kDtReset = 1.0e15;                 // cuf_kernel.cuf:790
+constexpr double kEpsB = 1.0e-6;                    // Solvers.f90:1195
+constexpr double kTtEps = 1.0e-9;                   // Solvers.f90:1625,1634
+
+enum : int { kFlagWave = 1, kFlagStar = 2 };
+
+// ------------------------------------------------------------------ elementary functions
+SB_HD double sb_sqrt(double x) { return sqrt(x); }
+SB_HD float sb_sqrt(float x) {
+#if defined(__CUDA_ARCH__)
+    return __fsqrt_rn(x);
+#else
+    return std::sqrt(x);
+#endif
+}
+SB_HD double sb_rcp(double x) {
+#if defined(__CUDA_ARCH__)
+    return __drcp_rn(x);
+#else
+    return 1.0 / x;
+#endif
+}
+SB_HD float sb_rcp(float x) {
+#if defined(__CUDA_ARCH__)
+    return __frcp_rn(x);
+#else
+    return 1.0f / x;
+#endif
+}
+SB_HD double sb_rsqrt(double x) {
+#if defined(__CUDA_ARCH__)
+    return rsqrt(x);
+#else
+    return 1.0 / std::sqrt(x);
+#endif
+}
+SB_HD float sb_rsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+    return rsqrtf(x);
+#else
+    return 1.0f / std::sqrt(x);
+#endif
+}
+template <typename T> SB_HD T sb_abs(T x) { return x < T(0) ? -x : x; }
+template <typename T> SB_HD T sb_min(T a, T b) { return b < a ? b : a; }
+template <typename T> SB_HD T sb_max(T a, T b) { return a < b ? b : a; }
+template <typename T> SB_HD T sb_pos(T x) { return x > T(0) ? x : T(0); }
+
+// Solvers.f90:126-137: (signum(x)+signum(y))/2 * min(|x|,|y|)
+template <typename T> SB_HD T minmod(T a, T b) {
+    if (a > T(0) && b > T(0)) return sb_min(a, b);
+    if (a < T(0) && b < T(0)) return sb_max(a, b);
+    return T(0);
+}
+
+// ------------------------------------------------------------------ conserved -> primitive
+// U = (rho, mx, my, mz, E, Bx, By, Bz), B in stored units, E carrying |B/sqrt(4pi)|^2/2.
+// Pressure recovery: p = ((E - rho|v|^2/2) - |b|^2/2)(gamma-1)  (cuf_solvers.cuf:735-738 with the
+// magnetic term of the conservative MHD energy).
+SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
+    const double rho = U[0];
+    const double ir = sb_rcp(rho);
+    const double u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
+    const double bx = U[5] * kInvSpi4, by = U[6] * kInvSpi4, bz = U[7] * kInvSpi4;
+    ke = 0.5 * rho * ((u * u + v * v) + w * w);
+    me = 0.5 * ((bx * bx + by * by) + bz * bz);
+    q[0] = rho;
+    q[1] = u;
+    q[2] = v;
+    q[3] = w;
+    q[4] = ((U[4] - ke) - me) * kG1;
+    q[5] = U[5];
+    q[6] = U[6];
+    q[7] = U[7];
+}
+
+// ------------------------------------------------------------------ Riemann solver
+// Face-frame states q = (rho, vn, vt1, vt2, p, Bn, Bt1, Bt2), B in stored units.
+// Output F in the same order (B fluxes in stored units, not multiplied by the face area),
+// SL, SR, SM (chlld's dsl, dsp, dsc).  wv is the face speed (used only when MOVING).
+// Returns a bit set: kFlagWave when no wave-fan region matched (the reference STOPs),
+// kFlagStar (CHECK_STAR only) when the selected state has rho <= 0 or p <= 0 or F is not finite.
+template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR>
+SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& SRo, T& SMo) {
+    const T ispi4 = T(kInvSpi4);
+    const T ga = T(kGamma);
+    const T ig1 = T(kInvG1);
+    const T g1 = T(kG1);
+    const T half = T(0.5);
+    if (!MOVING) wv = T(0);
+
+    const T r1 = q1[0], u1 = q1[1], v1 = q1[2], w1 = q1[3], p1 = q1[4];
+    const T bx1 = q1[5] * ispi4, by1 = q1[6] * ispi4, bz1 = q1[7] * ispi4;
+    const T r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
+    const T bx2 = q2[5] * ispi4, by2 = q2[6] * ispi4, bz2 = q2[7] * ispi4;
+
+    // fast magnetosonic speeds, Solvers.f90:1282-1306
+    const T ir1 = sb_rcp(r1), ir2 = sb_rcp(r2);
+    const T aaL = bx1 * sb_rsqrt(r1);
+    const T b2L = (bx1 * bx1 + by1 * by1) + bz1 * bz1;
+    const T b21 = b2L * ir1;
+    const T cL = sb_sqrt(ga * p1 * ir1);
+    const T cfL = half * (sb_sqrt(sb_pos(b21 + cL * (cL + T(2) * aaL))) +
+                          sb_sqrt(sb_pos(b21 + cL * (cL - T(2) * aaL))));
+    const T ptL = p1 + half * b2L;
+    const T aaR = bx2 * sb_rsqrt(r2);
+    const T b2R = (bx2 * bx2 + by2 * by2) + bz2 * bz2;
+    const T b22 = b2R * ir2;
+    const T cR = sb_sqrt(ga * p2 * ir2);
+    const T cfR = half * (sb_sqrt(sb_pos(b22 + cR * (cR + T(2) * aaR))) +
+                          sb_sqrt(sb_pos(b22 + cR * (cR - T(2) * aaR))));
+    const T ptR = p2 + half * b2R;
+
+    // wave-speed estimates, :1308-1330
+    T SL = sb_min(u1 - cfL, u2 - cfR);
+    T SR = sb_max(u1 + cfL, u2 + cfR);
+    T cfC = T(0), vC1 = T(0);
+    if (n_disc != 0 || NSTATE == 0) {
+        const T aC = half * (aaL + aaR);
+        const T b2o = half * (b22 + b21);
+        const T cC = sb_sqrt(ga * (half * (p2 + p1)) * sb_rcp(half * (r2 + r1)));
+        cfC = half * (sb_sqrt(sb_pos(b2o + cC * (cC + T(2) * aC))) +
+                      sb_sqrt(sb_pos(b2o + cC * (cC - T(2) * aC))));
+        vC1 = half * (u1 + u2);
+        if (n_disc == 1) {
+            SL = sb_min(u1 - cfL, vC1 - cfC);
+            SR = sb_max(u2 + cfR, vC1 + cfC);
+        } else if (n_disc == 2) {
+            const T SL1 = sb_min(u1 - cfL, vC1 - cfC), SR1 = sb_max(u2 + cfR, vC1 + cfC);
+            const T SL2 = sb_min(u1 - cfL, u2 - cfR), SR2 = sb_max(u1 + cfL, u2 + cfR);
+            SL = T(0.75) * SL1 + T(0.25) * SL2;
+            SR = T(0.75) * SR1 + T(0.25) * SR2;
+        }
+    }
+    const T suR = SR - u2, suL = SL - u1;
+    const T idd = sb_rcp(suR * r2 - suL * r1);
+    const T SM = (((suR * r2 * u2 - ptR) + ptL) - suL * r1 * u1) * idd;
+    SLo = SL;
+    SRo = SR;
+    SMo = SM;
+    if (NSTATE == 0) {   // one-speed Lax, :1360-1365
+        const T TR0 = sb_abs(u1 + u2) * half + cfC;
+        SL = -TR0;
+        SR = TR0;
+    }
+
+    // left/right energies, fluxes and conserved vectors, :1368-1404
+    const T e1 = (p1 * ig1 + r1 * (half * ((u1 * u1 + v1 * v1) + w1 * w1))) + half * b2L;
+    const T e2 = (p2 * ig1 + r2 * (half * ((u2 * u2 + v2 * v2) + w2 * w2))) + half * b2R;
+    const T sbv1 = (u1 * bx1 + v1 * by1) + w1 * bz1;
+    const T sbv2 = (u2 * bx2 + v2 * by2) + w2 * bz2;
+    const T m1 = r1 * u1, m2 = r2 * u2;
+    T FL[8], FR[8], UL[8], UR[8];
+    FL[0] = m1;
+    FL[1] = (m1 * u1 + ptL) - bx1 * bx1;
+    FL[2] = m1 * v1 - bx1 * by1;
+    FL[3] = m1 * w1 - bx1 * bz1;
+    FL[4] = (e1 + ptL) * u1 - bx1 * sbv1;
+    FL[5] = T(0);
+    FL[6] = u1 * by1 - v1 * bx1;
+    FL[7] = u1 * bz1 - w1 * bx1;
+    FR[0] = m2;
+    FR[1] = (m2 * u2 + ptR) - bx2 * bx2;
+    FR[2] = m2 * v2 - bx2 * by2;
+    FR[3] = m2 * w2 - bx2 * bz2;
+    FR[4] = (e2 + ptR) * u2 - bx2 * sbv2;
+    FR[5] = T(0);
+    FR[6] = u2 * by2 - v2 * bx2;
+    FR[7] = u2 * bz2 - w2 * bx2;
+    UL[0] = r1; UL[1] = m1; UL[2] = r1 * v1; UL[3] = r1 * w1; UL[4] = e1;
+    UL[5] = bx1; UL[6] = by1; UL[7] = bz1;
+    UR[0] = r2; UR[1] = m2; UR[2] = r2 * v2; UR[3] = r2 * w2; UR[4] = e2;
+    UR[5] = bx2; UR[6] = by2; UR[7] = bz2;
+
+    int flag = 0;
+    const T isrl = sb_rcp(SR - SL);
+    // HLL average of the normal field, UZ(6) (:1406-1408 with FL(6) = FR(6) = 0)
+    const T bn = (SR * bx2 - SL * bx1) * isrl;
+
+    if (NSTATE <= 1) {   // :1414-1463
+        T TL = SL, TR = SR;
+        if (SL > wv) TL = T(0);
+        if (SR < wv) TR = T(0);
+        const T a = TR * TL;
+        const T ib = sb_rcp(TR - TL);
+#pragma unroll
+        for (int k = 0; k < 8; k++) F[k] = ((TR * FL[k] - TL * FR[k]) + a * (UR[k] - UL[k])) * ib;
+        if (MOVING) {
+            // FW: last matching block wins (:1422-1438)
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                T fw;
+                if (SR < wv) fw = wv * UR[k];
+                else if (SL <= wv && wv <= SR) fw = wv * ((SR * UR[k] - SL * UL[k] + FL[k] - FR[k]) * isrl);
+                else fw = wv * UL[k];
+                F[k] = F[k] - fw;
+            }
+        }
+        if (!(SL > wv) && !(SL <= wv && wv <= SR) && !(SR < wv)) flag |= kFlagWave;
+    } else {
+        const T isrm = sb_rcp(SR - SM), islm = sb_rcp(SL - SM);
+        const T suRm = suR * isrm, suLm = suL * islm;
+        const T rzR = r2 * suRm, rzL = r1 * suLm;
+        T vzL2, vzL3, vzR2, vzR3, bzL2, bzL3, bzR2, bzR3, ezL, ezR;
+        // selected-region coefficients: F = Fs + a2*(UZZs - UZs) + a1*(UZs - Us) - wv*Wsel
+        int region;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
+        T vzz2 = T(0), vzz3 = T(0), bzz2 = T(0), bzz3 = T(0), ezzL = T(0), ezzR = T(0);
+        T SZL = SM, SZR = SM;
+        bool ibn = false;
+        if (NSTATE == 2) {   // HLLC, :1465-1567
+            const T ptz = half * ((ptR + r2 * suR * (SM - u2)) + (ptL + r1 * suL * (SM - u1)));
+            const T uz0 = ((SR * r2 - SL * r1) + FL[0] - FR[0]) * isrl;
+            const T uz1 = ((SR * UR[1] - SL * UL[1]) + FL[1] - FR[1]) * isrl;
+            const T uz2 = ((SR * UR[2] - SL * UL[2]) + FL[2] - FR[2]) * isrl;
+            const T uz3 = ((SR * UR[3] - SL * UL[3]) + FL[3] - FR[3]) * isrl;
+            const T uz6 = ((SR * by2 - SL * by1) + FL[6] - FR[6]) * isrl;
+            const T uz7 = ((SR * bz2 - SL * bz1) + FL[7] - FR[7]) * isrl;
+            const T sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * sb_rcp(uz0);
+            ezR = e2 * suRm + (((ptz * SM - ptR * u2) + bn * (sbv2 - sbvz)) * isrm);
+            ezL = e1 * suLm + (((ptz * SM - ptL * u1) + bn * (sbv1 - sbvz)) * islm);
+            if (sb_abs(bn) < T(kEpsB)) {
+                vzR2 = v2; vzR3 = w2; vzL2 = v1; vzL3 = w1;
+                bzR2 = by2 * suRm; bzR3 = bz2 * suRm;
+                bzL2 = by1 * suLm; bzL3 = bz1 * suLm;
+            } else {
+                const T cR = bn * sb_rcp(suR * r2), cL = bn * sb_rcp(suL * r1);
+                vzR2 = v2 + (by2 - uz6) * cR;
+                vzR3 = w2 + (bz2 - uz7) * cR;
+                vzL2 = v1 + (by1 - uz6) * cL;
+                vzL3 = w1 + (bz1 - uz7) * cL;
+                bzR2 = uz6; bzR3 = uz7; bzL2 = uz6; bzL3 = uz7;
+            }
+            if (SR < wv) region = 6;
+            else if (SM <= wv && SR >= wv) region = 5;
+            else if (SL <= wv && SM >= wv) region = 2;
+            else if (SL > wv) region = 1;
+            else region = 0;
+        } else {             // HLLD, :1598-1814
+            const T ptz = ((suR * r2 * ptL - suL * r1 * ptR) + r1 * r2 * suR * suL * (u2 - u1)) * idd;
+            const T bn2 = bn * bn;
+            T tvR = T(0), tbR = T(0), tvL = T(0), tbL = T(0);
+            const T ttR = r2 * suR * (SR - SM) - bn2;
+            if (!(sb_abs(ttR) <= T(kTtEps))) {
+                const T i = sb_rcp(ttR);
+                tvR = (SM - u2) * i;
+                tbR = (r2 * suR * suR - bn2) * i;
+            }
+            const T ttL = r1 * suL * (SL - SM) - bn2;
+            if (!(sb_abs(ttL) <= T(kTtEps))) {
+                const T i = sb_rcp(ttL);
+                tvL = (SM - u1) * i;
+                tbL = (r1 * suL * suL - bn2) * i;
+            }
+            vzL2 = v1 - bn * by1 * tvL;
+            vzL3 = w1 - bn * bz1 * tvL;
+            vzR2 = v2 - bn * by2 * tvR;
+            vzR3 = w2 - bn * bz2 * tvR;
+            bzL2 = by1 * tbL;
+            bzL3 = bz1 * tbL;
+            bzR2 = by2 * tbR;
+            bzR3 = bz2 * tbR;
+            const T sbvL = (bn * SM + bzL2 * vzL2) + bzL3 * vzL3;
+            const T sbvR = (bn * SM + bzR2 * vzR2) + bzR3 * vzR3;
+            ezR = e2 * suRm + (((ptz * SM - ptR * u2) + bn * (sbv2 - sbvR)) * isrm);
+            ezL = e1 * suLm + (((ptz * SM - ptL * u1) + bn * (sbv1 - sbvL)) * islm);
+            const T rzRs = sb_sqrt(rzR), rzLs = sb_sqrt(rzL);
+            const T abn = sb_abs(bn);
+            T sbn = T(0);
+            if (abn > T(kEpsB)) {
+                ibn = true;
+                sbn = bn > T(0) ? T(1) : T(-1);
+                SZL = SM - abn * sb_rcp(rzLs);
+                SZR = SM + abn * sb_rcp(rzRs);
+            }
+            const T irzss = sb_rcp(rzRs + rzLs);
+            const T rzps = rzRs * rzLs;
+            vzz2 = ((rzLs * vzL2 + rzRs * vzR2) + sbn * (bzR2 - bzL2)) * irzss;
+            vzz3 = ((rzLs * vzL3 + rzRs * vzR3) + sbn * (bzR3 - bzL3)) * irzss;
+            bzz2 = ((rzLs * bzR2 + rzRs * bzL2) + sbn * rzps * (vzR2 - vzL2)) * irzss;
+            bzz3 = ((rzLs * bzR3 + rzRs * bzL3) + sbn * rzps * (vzR3 - vzL3)) * irzss;
+            const T sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
+            ezzR = ezR + rzRs * sbn * (sbvR - sbzz);
+            ezzL = ezL - rzLs * sbn * (sbvL - sbzz);
+            if (SR < wv) region = 6;
+            else if (SZR <= wv && SR >= wv) region = 5;
+            else if (ibn && SM <= wv && SZR >= wv) region = 4;
+            else if (ibn && SZL <= wv && SM >= wv) region = 3;
+            else if (SL <= wv && SZL >= wv) region = 2;
+            else if (SL > wv) region = 1;
+            else region = 0;
+        }
+        if (region == 0) flag |= kFlagWave;
+        const bool right = region >= 4;
+        // selected side (element-wise selects keep FL/FR/UL/UR in registers)
+        const T rz = right ? rzR : rzL;
+        const T S1 = right ? SR : SL;
+        const T S2 = right ? SZR : SZL;
+        const T vz2 = right ? vzR2 : vzL2, vz3 = right ? vzR3 : vzL3;
+        const T bz2_ = right ? bzR2 : bzL2, bz3_ = right ? bzR3 : bzL3;
+        const T ez = right ? ezR : ezL, ezz = right ? ezzR : ezzL;
+        T UZs[8], UZZs[8];
+        UZs[0] = rz; UZs[1] = rz * SM; UZs[2] = rz * vz2; UZs[3] = rz * vz3; UZs[4] = ez;
+        UZs[5] = bn; UZs[6] = bz2_; UZs[7] = bz3_;
+        UZZs[0] = rz; UZZs[1] = rz * SM; UZZs[2] = rz * vzz2; UZZs[3] = rz * vzz3; UZZs[4] = ezz;
+        UZZs[5] = bn; UZZs[6] = bzz2; UZZs[7] = bzz3;
+        const bool use1 = (region == 2 || region == 3 || region == 4 || region == 5);
+        const bool use2 = (region == 3 || region == 4);
+        T W[8];   // the state whose flux is returned (for the face-speed term and the check)
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const T us = right ? UR[k] : UL[k];
+            T f = right ? FR[k] : FL[k];
+            if (use2) f = f + S2 * (UZZs[k] - UZs[k]);
+            if (use1) f = f + S1 * (UZs[k] - us);
+            W[k] = use2 ? UZZs[k] : (use1 ? UZs[k] : us);
+            if (MOVING) f = f - wv * W[k];
+            F[k] = f;
+        }
+        if (CHECK_STAR) {
+            const T iw = sb_rcp(W[0]);
+            const T pstar = ((W[4] - half * ((W[1] * W[1] + W[2] * W[2]) + W[3] * W[3]) * iw) -
+                             half * ((W[5] * W[5] + W[6] * W[6]) + W[7] * W[7])) * g1;
+            if (!(W[0] > T(0)) || !(pstar > T(0))) flag |= kFlagStar;
+        }
+        // normal-field flux, :1570-1581 / :1828-1839
+        const T SN = sb_max(sb_abs(SL), sb_abs(SR));
+        T wbn = T(0);
+        if (MOVING) {
+            if (wv >= SR) wbn = wv * bx2;
+            else if (wv <= SL) wbn = wv * bx1;
+            else wbn = wv * (bx1 + bx2) * half;
+        }
+        F[5] = -SN * (bx2 - bx1) - wbn;
+    }
+    // B fluxes back to stored units (:1846)
+    const T spi4 = T(kSpi4);
+    F[5] *= spi4;
+    F[6] *= spi4;
+    F[7] *= spi4;
+    if (CHECK_STAR) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if (!(sb_abs(F[k]) < T(3.0e38))) flag |= kFlagStar;
+    }
+    return flag;
+}
+
+// MUSCL-minmod face value of cell c toward its neighbour n with the far cell f on the other
+// side: t_c + 0.5*minmod(t_c - t_f, t_n - t_c).  On the Cartesian grid this is the reference's
+// linear(-3h/2, t_f, -h/2, t_c, h/2, t_n, 0) (Solvers.f90:141-150, cuf_solvers.cuf:389-392).
+template <typename T> SB_HD T muscl(T tf, T tc, T tn) { return tc + T(0.5) * minmod(tc - tf, tn - tc); }
+
+// Face states from the 4-cell stencil (face-frame order), with the positivity fallback of
+// cuf_solvers.cuf:394-406.  Only rho, vn, vt1, vt2, p are reconstructed; B stays first order.
+template <typename T, int ORDER>
+SB_HD void reconstruct(const T* qLL, const T* qL, const T* qR, const T* qRR, T* q1, T* q2) {
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        q1[v] = qL[v];
+        q2[v] = qR[v];
+    }
+    if (ORDER == 2) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+            q1[v] = muscl(qLL[v], qL[v], qR[v]);
+            q2[v] = muscl(qRR[v], qR[v], qL[v]);
+        }
+        if (q1[0] < T(0)) q1[0] = qL[0];
+        if (q1[4] < T(0)) q1[4] = qL[4];
+        if (q2[0] < T(0)) q2[0] = qR[0];
+        if (q2[4] < T(0)) q2[4] = qR[4];
+    }
+}
+
+}  // namespace sb

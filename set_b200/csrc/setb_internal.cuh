@@ -1,0 +1,255 @@
+// setb_internal.cuh -- device-side structures shared by the stage kernels and the host runtime.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "mhd_core.cuh"
+
+namespace sb {
+
+// Clock of one solve, in device memory.  The reference keeps time_step / time_step2 /
+// dev_time_all as device scalars written from the host each step (cuf_kernel.cuf:18-19,
+// 789-794); here the last CTA of each step's final kernel rolls the clock on the device, so a
+// run of steps needs no host round trip.
+struct DevClock {
+    double dt_cur;                  // dt used by the current step (time_step)
+    unsigned long long dt_next;     // bits of the running min for the next step (time_step2)
+    double time_all;                // dev_time_all
+    double dt_last;                 // dt used by the previous step
+    unsigned int counter;           // CTAs finished in the running kernel
+    unsigned int pad;
+    long long steps;
+};
+
+struct DevStatus {
+    unsigned long long n_negdens, n_pfloor, n_wave, n_recon, n_redo;
+    unsigned long long first_bad;   // ULLONG_MAX when none
+};
+
+// Geometry + boundary data of one Cartesian grid.
+struct GridGeom {
+    int nx, ny, nz, lz;             // lz: z extent of one CTA's march
+    long long vs, ps, px;           // var / plane / row strides of the SoA state (elements)
+    double lo[3], h[3];
+    double square[3];               // face areas: hy*hz, hx*hz, hx*hy
+    double inv_vol;                 // 1/(hx*hy*hz)
+    double inv_dist[3];             // 1/(h/2)
+    double inflow[8];               // primitive ghost state beyond x = hi
+    double r_src, rho_src, v_src, p_over_rho_src, r_floor;
+};
+
+struct StageArgs {
+    GridGeom g;
+    const double* __restrict__ Uin;     // state the fluxes are computed from
+    const double* Ubase;                // stage 2: U^n (may alias Uout: read before written, same thread)
+    double* Uout;
+    DevClock* clk;
+    DevStatus* st;
+    double cfl;
+    int n_disc;
+    int finalize;                       // last CTA rolls the clock (Euler, or Heun stage 2)
+};
+
+// Geometry of cell centres, evaluated with explicitly rounded operations so that host, device
+// and every kernel agree bit for bit (FMA contraction would change the source-sphere test).
+SB_HD double cell_coord(double lo, int i, double h) {
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(lo, __dmul_rn((double)i + 0.5, h));
+#else
+    return lo + ((double)i + 0.5) * h;
+#endif
+}
+SB_HD double dmul(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+SB_HD double dadd(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+SB_HD double dsub(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+
+// Conserved state from a primitive one, exactly rounded (no contraction): used for initial
+// conditions, the re-imposed source state and Cell_par uploads.
+SB_HD void cons_from_prim_exact(const double* q, double* U) {
+    const double rho = q[0], u = q[1], v = q[2], w = q[3];
+    const double bx = q[5] / kSpi4, by = q[6] / kSpi4, bz = q[7] / kSpi4;
+    const double ke = dmul(dmul(0.5, rho), dadd(dadd(dmul(u, u), dmul(v, v)), dmul(w, w)));
+    const double me = dmul(0.5, dadd(dadd(dmul(bx, bx), dmul(by, by)), dmul(bz, bz)));
+    U[0] = rho;
+    U[1] = dmul(rho, u);
+    U[2] = dmul(rho, v);
+    U[3] = dmul(rho, w);
+    U[4] = dadd(dadd(q[4] / kG1, ke), me);
+    U[5] = q[5];
+    U[6] = q[6];
+    U[7] = q[7];
+}
+
+// Primitive state from a conserved one, exactly rounded with true divisions (Cell_par downloads).
+SB_HD void prim_from_cons_exact(const double* U, double* q) {
+    const double rho = U[0];
+    const double u = U[1] / rho, v = U[2] / rho, w = U[3] / rho;
+    const double bx = U[5] / kSpi4, by = U[6] / kSpi4, bz = U[7] / kSpi4;
+    const double ke = dmul(dmul(0.5, rho), dadd(dadd(dmul(u, u), dmul(v, v)), dmul(w, w)));
+    const double me = dmul(0.5, dadd(dadd(dmul(bx, bx), dmul(by, by)), dmul(bz, bz)));
+    q[0] = rho;
+    q[1] = u;
+    q[2] = v;
+    q[3] = w;
+    q[4] = dmul(dsub(dsub(U[4], ke), me), kG1);
+    q[5] = U[5];
+    q[6] = U[6];
+    q[7] = U[7];
+}
+
+// Source state (primitive) at cell (i,j,k); false when the cell is outside r_src.
+SB_HD bool source_prim(const GridGeom& g, int i, int j, int k, double* q) {
+    if (!(g.r_src > 0.0)) return false;
+    const double x = cell_coord(g.lo[0], i, g.h[0]);
+    const double y = cell_coord(g.lo[1], j, g.h[1]);
+    const double z = cell_coord(g.lo[2], k, g.h[2]);
+    const double r2 = dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
+    if (!(r2 < dmul(g.r_src, g.r_src))) return false;
+    const double r = sqrt(r2);
+    const double re = r > g.r_floor ? r : g.r_floor;
+    const double s = g.r_src / re;
+    const double rho = dmul(dmul(s, s), g.rho_src);
+    q[0] = rho;
+    if (r > 0.0) {
+        q[1] = dmul(g.v_src, x / r);
+        q[2] = dmul(g.v_src, y / r);
+        q[3] = dmul(g.v_src, z / r);
+    } else {
+        q[1] = q[2] = q[3] = 0.0;
+    }
+    q[4] = dmul(g.p_over_rho_src, rho);
+    q[5] = q[6] = q[7] = 0.0;
+    return true;
+}
+
+SB_HD uint64_t splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+SB_HD double unit_draw(uint64_t seed, uint64_t cell, uint64_t which) {
+    const uint64_t hsh = splitmix64(splitmix64(seed) ^ (2 * cell + which));
+    return dmul((double)(hsh >> 11), 1.0 / 9007199254740992.0);
+}
+
+// Seeded initial condition of one cell (primitive).
+SB_HD void lism_prim(const GridGeom& g, const double* lism, uint64_t seed, double pert, int i, int j,
+                     int k, double* q) {
+    if (!source_prim(g, i, j, k, q)) {
+        const uint64_t c = (uint64_t)i + (uint64_t)g.nx * ((uint64_t)j + (uint64_t)g.ny * (uint64_t)k);
+        const double d1 = dmul(pert, dsub(dmul(2.0, unit_draw(seed, c, 0)), 1.0));
+        const double d2 = dmul(pert, dsub(dmul(2.0, unit_draw(seed, c, 1)), 1.0));
+        q[0] = dmul(lism[0], dadd(1.0, d1));
+        q[1] = lism[1];
+        q[2] = lism[2];
+        q[3] = lism[3];
+        q[4] = dmul(lism[4], dadd(1.0, d2));
+        q[5] = lism[5];
+        q[6] = lism[6];
+        q[7] = lism[7];
+    }
+}
+
+// Seeded initial condition of one cell (conserved).
+SB_HD void lism_cell(const GridGeom& g, const double* lism, uint64_t seed, double pert, int i, int j,
+                     int k, double* U) {
+    double q[8];
+    lism_prim(g, lism, seed, pert, i, j, k, q);
+    cons_from_prim_exact(q, U);
+}
+
+// General-normal chlld for a batch of faces: the lab states are rotated into an orthonormal
+// face frame (the reference's basis construction, Solvers.f90:1236-1273), solved, and the
+// momentum / B fluxes rotated back.
+template <typename T, int NSTATE>
+SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const double* q2d, int n_disc,
+                          double* qqq, double* sp, int32_t* flag) {
+    const double al = nrm[0], be = nrm[1], ge = nrm[2];
+    double bav[3];
+    for (int c = 0; c < 3; c++) bav[c] = 0.5 * (q1d[5 + c] + q2d[5 + c]) * kInvSpi4;
+    const double bk = bav[0] * al + bav[1] * be + bav[2] * ge;
+    double d = (bav[0] * bav[0] + bav[1] * bav[1] + bav[2] * bav[2]) - bk * bk;
+    double e2[3], e3[3];
+    if (d > 1.0e-12) {
+        d = sqrt(d);
+        e2[0] = (bav[0] - bk * al) / d;
+        e2[1] = (bav[1] - bk * be) / d;
+        e2[2] = (bav[2] - bk * ge) / d;
+        e3[0] = (bav[1] * ge - bav[2] * be) / d;
+        e3[1] = (bav[2] * al - bav[0] * ge) / d;
+        e3[2] = (bav[0] * be - bav[1] * al) / d;
+    } else {
+        double ai[3] = {0.0, 0.0, 0.0};
+        if (sb_abs(al) < sb_abs(be) && sb_abs(al) < sb_abs(ge)) ai[0] = 1.0;
+        else if (sb_abs(be) < sb_abs(ge)) ai[1] = 1.0;
+        else ai[2] = 1.0;
+        const double aik = ai[0] * al + ai[1] * be + ai[2] * ge;
+        d = sqrt(1.0 - aik * aik);
+        e2[0] = (ai[0] - aik * al) / d;
+        e2[1] = (ai[1] - aik * be) / d;
+        e2[2] = (ai[2] - aik * ge) / d;
+        e3[0] = (ai[1] * ge - ai[2] * be) / d;
+        e3[1] = (ai[2] * al - ai[0] * ge) / d;
+        e3[2] = (ai[0] * be - ai[1] * al) / d;
+    }
+    T a[8], b[8], F[8], SL, SR, SM;
+    const double* qs[2] = {q1d, q2d};
+    T* outs[2] = {a, b};
+    for (int s = 0; s < 2; s++) {
+        const double* q = qs[s];
+        T* o = outs[s];
+        o[0] = T(q[0]);
+        o[4] = T(q[4]);
+        o[1] = T(q[1] * al + q[2] * be + q[3] * ge);
+        o[2] = T(q[1] * e2[0] + q[2] * e2[1] + q[3] * e2[2]);
+        o[3] = T(q[1] * e3[0] + q[2] * e3[1] + q[3] * e3[2]);
+        o[5] = T(q[5] * al + q[6] * be + q[7] * ge);
+        o[6] = T(q[5] * e2[0] + q[6] * e2[1] + q[7] * e2[2]);
+        o[7] = T(q[5] * e3[0] + q[6] * e3[1] + q[7] * e3[2]);
+    }
+    const int fl = riemann<T, NSTATE, true, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
+    qqq[0] = F[0];
+    qqq[4] = F[4];
+    const double nn[3] = {al, be, ge};
+    for (int c = 0; c < 3; c++) {
+        qqq[1 + c] = nn[c] * (double)F[1] + e2[c] * (double)F[2] + e3[c] * (double)F[3];
+        qqq[5 + c] = nn[c] * (double)F[5] + e2[c] * (double)F[6] + e3[c] * (double)F[7];
+    }
+    sp[0] = SL;
+    sp[1] = SR;
+    sp[2] = SM;
+    *flag = fl;
+}
+
+// ---------------------------------------------------------------- launch entry points
+cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int kind, bool want_dt,
+                              cudaStream_t s);
+cudaError_t launch_lism_init(const GridGeom& g, const double* lism, uint64_t seed, double pert,
+                             double* U, cudaStream_t s);
+cudaError_t launch_prim_to_cons(const GridGeom& g, const double* prim8, double* U, cudaStream_t s);
+cudaError_t launch_cons_to_prim(const GridGeom& g, const double* U, double* prim8, cudaStream_t s);
+cudaError_t launch_chlld_batch(int64_t n, int n_state, int n_disc, int precision,
+                               const double* normals, const double* w, const double* q1,
+                               const double* q2, double* qqq, double* speeds, int32_t* flags,
+                               cudaStream_t s);
+int stage_fp64_smem_bytes();
+
+}  // namespace sb

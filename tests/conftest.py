@@ -1,0 +1,31 @@
+"""Shared test set-up: repo root on sys.path, the `gpu` marker, and in-tree builds."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the CUDA path through the C ABI")
+
+
+@pytest.fixture(scope="session", autouse=True)
+def _built():
+    """Build the oracle (checker) and the product library in-tree if they are stale."""
+    import oracle
+    oracle.build()
+    from set_b200 import build
+    build.build()
+    yield
+
+
+def has_gpu() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False

@@ -1,0 +1,207 @@
+"""GPU parity of the CUDA path against the CPU FP64 oracle, through the C ABI.
+
+Tolerances (plain FP64 form):
+  * one step from identical input: |U_gpu - U_oracle| <= 1e-12 * max(|U_oracle|, 1e-6 * max|U_oracle,v|)
+    for every cell and conserved variable v;
+  * after 100 steps: relative L1 error sum|dU_v| / sum|U_v| <= 1e-10 for every conserved variable;
+  * initial conditions, Cell_par conversions and the source state: bit-identical.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import set_b200 as S
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-12
+L1_TOL = 1e-10
+
+
+def oracle_problem(desc, ic):
+    g = O.make_grid((desc.nx, desc.ny, desc.nz), inflow=np.array(desc.inflow[:]), r_src=desc.r_src,
+                    rho_src=desc.rho_src, v_src=desc.v_src, p_over_rho_src=desc.p_over_rho_src,
+                    r_floor=desc.r_floor, dt_init=desc.dt_init)
+    U = O.init_lism(g, lism=np.array(ic.lism[:]), seed=ic.seed, pert_amp=ic.pert_amp)
+    return g, U
+
+
+def oracle_opts(o):
+    return O.make_opts(o.n_state, o.order, o.scheme, o.cfl, o.n_disc)
+
+
+def step_err(Ug, Uo):
+    floor = 1e-6 * np.abs(Uo).reshape(8, -1).max(axis=1)
+    den = np.maximum(np.abs(Uo), floor[:, None, None, None])
+    return (np.abs(Ug - Uo) / den).reshape(8, -1).max(axis=1)
+
+
+def l1_err(Ug, Uo):
+    return np.abs(Ug - Uo).reshape(8, -1).sum(axis=1) / np.maximum(np.abs(Uo).reshape(8, -1).sum(axis=1), 1e-300)
+
+
+def rand_state(rng, bscale=2.0):
+    return np.array([rng.uniform(0.1, 4.0), *rng.normal(0, 1.5, 3), rng.uniform(0.05, 4.0),
+                     *rng.normal(0, bscale, 3)])
+
+
+# ------------------------------------------------------------------ the solver core
+@pytest.mark.parametrize("n_state", [0, 1, 2, 3])
+def test_chlld_batch_fp64_matches_oracle(n_state):
+    rng = np.random.default_rng(300 + n_state)
+    n = 4000
+    q1 = np.array([rand_state(rng, 0.0 if n_state == 2 else 2.0) for _ in range(n)])
+    q2 = np.array([rand_state(rng, 0.0 if n_state == 2 else 2.0) for _ in range(n)])
+    nr = rng.normal(size=(n, 3))
+    nr[: n // 2] = np.eye(3)[rng.integers(0, 3, n // 2)] * rng.choice([-1.0, 1.0], (n // 2, 1))
+    nr /= np.linalg.norm(nr, axis=1, keepdims=True)
+    w = np.where(np.arange(n) % 3 == 0, rng.normal(size=n), 0.0)
+    qqq, sp, fl = S.chlld_batch(n_state, nr, q1, q2, w=w)
+    assert (fl & 1).sum() == 0
+    for k in range(n):
+        rc, g, sl, sr, sm = O.chlld(n_state, nr[k], w[k], q1[k], q2[k])
+        assert rc == 0
+        assert np.abs(qqq[k] - g).max() <= 1e-12 * np.abs(g).max(), k
+        assert abs(sp[k, 0] - sl) <= 1e-12 * max(1.0, abs(sl)) and abs(sp[k, 1] - sr) <= 1e-12 * max(1.0, abs(sr))
+
+
+def test_chlld_batch_reference_golden_hll():
+    g = np.load(__file__.replace("test_gpu_parity.py", "golden/gelios_hll.npz"))
+    qqq, sp, fl = S.chlld_batch(1, g["normal"], g["q1"], g["q2"], w=g["w"])
+    err = np.abs(qqq - g["qqq"]).max(axis=1) / np.abs(g["qqq"]).max(axis=1)
+    assert err.max() <= 1e-12
+
+
+def test_chlld_batch_fp32_close_to_fp64():
+    # the mixed form's Riemann arithmetic: FP32, judged against the FP64 oracle
+    rng = np.random.default_rng(17)
+    n = 3000
+    q1 = np.array([rand_state(rng) for _ in range(n)])
+    q2 = np.array([rand_state(rng) for _ in range(n)])
+    nr = np.eye(3)[rng.integers(0, 3, n)]
+    q32, _, fl = S.chlld_batch(3, nr, q1, q2, precision=1)
+    q64, _, _ = S.chlld_batch(3, nr, q1, q2, precision=0)
+    ok = (fl == 0)
+    err = np.abs(q32 - q64).max(axis=1) / np.abs(q64).max(axis=1)
+    assert ok.mean() > 0.95
+    assert np.median(err[ok]) < 1e-5 and err[ok].max() < 1e-2
+
+
+# ------------------------------------------------------------------ state, conversions, IC
+@pytest.mark.parametrize("n", [(20, 18, 16), (15, 15, 15)])
+def test_initial_condition_device_matches_oracle_bitwise(n):
+    desc = S.cart_desc(n)
+    ic = S.lism_ic(seed=4)
+    g, Uo = oracle_problem(desc, ic)
+    with S.Solver(desc, ic=ic) as s:
+        np.testing.assert_array_equal(s.conserved(), Uo)
+    with S.Solver(desc, cell_par=S.fill_lism(desc, ic)) as s:   # Set_CUDA path
+        np.testing.assert_array_equal(s.conserved(), Uo)
+
+
+def test_get_state_matches_oracle_conversion_and_keeps_columns_9_16():
+    desc = S.cart_desc((12, 11, 10))
+    ic = S.lism_ic(seed=5)
+    with S.Solver(desc, ic=ic) as s:
+        s.step(3, S.step_opts())
+        U = s.conserved()
+        cp = np.full((desc.nx * desc.ny * desc.nz, 16), 7.25)
+        cp, t = s.get_state(cp)
+        np.testing.assert_array_equal(cp[:, :8], O.cons_to_cellpar(U)[:, :8])
+        assert (cp[:, 8:] == 7.25).all()
+        assert t > 0
+        s.set_state(cp, 1.5)   # restart point: time set, dt reset to dt_init
+        d = s.status()
+        assert d.time_all == 1.5 and d.steps == 0 and d.dt_next == desc.dt_init
+
+
+# ------------------------------------------------------------------ one step, many shapes
+CASES = [
+    # (shape, n_state, order, scheme, lism kwargs)
+    ((20, 18, 16), 3, 2, 2, {}),
+    ((33, 9, 40), 3, 2, 2, {"tilt_deg": 30.0}),
+    ((15, 15, 15), 3, 2, 2, {}),                   # odd: a cell centred on the origin
+    ((24, 20, 18), 2, 2, 2, {"bmag": 0.0}),        # hydro: HLLC
+    ((20, 16, 12), 3, 1, 1, {}),                   # first order, forward Euler (config C1)
+    ((1, 16, 12), 3, 2, 2, {}),                    # one cell thick
+    ((70, 10, 9), 1, 2, 2, {}),                    # HLL, several column tiles in x
+    ((16, 16, 16), 0, 2, 2, {}),                   # one-speed Lax
+]
+
+
+@pytest.mark.parametrize("shape,n_state,order,scheme,lk", CASES)
+def test_one_step_matches_oracle(shape, n_state, order, scheme, lk):
+    inflow = S.lism_prim(**lk)
+    desc = S.cart_desc(shape, inflow=inflow, dt_init=2e-3)
+    ic = S.lism_ic(lism=inflow, seed=11)
+    o = S.step_opts(n_state=n_state, order=order, scheme=scheme)
+    g, Uo = oracle_problem(desc, ic)
+    ck, dgo = O.run(g, oracle_opts(o), Uo, 1)
+    with S.Solver(desc, ic=ic) as s:
+        t = s.step(1, o)
+        Ug = s.conserved()
+        d = s.status()
+    assert step_err(Ug, Uo).max() <= STEP_TOL, step_err(Ug, Uo)
+    assert t == ck.time_all
+    assert abs(d.dt_next - ck.dt_next) <= 1e-12 * ck.dt_next
+    assert d.n_negdens == dgo.n_negdens == 0
+    assert d.n_pfloor == dgo.n_pfloor
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (40, 24, 36)])
+def test_100_steps_l1_matches_oracle(shape):
+    desc = S.cart_desc(shape)
+    ic = S.lism_ic(seed=2)
+    o = S.step_opts()
+    g, Uo = oracle_problem(desc, ic)
+    ck, dgo = O.run(g, oracle_opts(o), Uo, 100)
+    with S.Solver(desc, ic=ic) as s:
+        t = s.step(100, o)
+        Ug = s.conserved()
+    e = l1_err(Ug, Uo)
+    assert e.max() <= L1_TOL, e
+    assert abs(t - ck.time_all) <= 1e-12 * ck.time_all
+
+
+# ------------------------------------------------------------------ physics properties
+@pytest.mark.parametrize("n_state,order,scheme", [(3, 2, 2), (2, 1, 1)])
+def test_conserves_mass_and_energy(n_state, order, scheme):
+    q = S.lism_prim(u=(0.3, -0.2, 0.1), bmag=0.0 if n_state == 2 else 1.0)
+    desc = S.cart_desc(24, inflow=q, r_src=0.0, dt_init=2e-3)
+    g, U = oracle_problem(desc, S.lism_ic(lism=q, pert_amp=0.0))
+    z, y, x = np.meshgrid(*(np.arange(24),) * 3, indexing="ij")
+    blob = np.clip(1.0 - ((x - 11.5) ** 2 + (y - 11.5) ** 2 + (z - 11.5) ** 2) / 16.0, 0.0, None) ** 2
+    U[0] *= 1.0 + 0.3 * blob
+    U[4] *= 1.0 + 0.5 * blob
+    cp = O.cons_to_cellpar(U)
+    with S.Solver(desc, cell_par=cp) as s:
+        U0 = s.conserved()
+        s.step(2 if scheme == 2 else 4, S.step_opts(n_state=n_state, order=order, scheme=scheme))
+        U1 = s.conserved()
+    for v in (0, 4):
+        assert abs(U1[v].sum() - U0[v].sum()) / U0[v].sum() < 1e-13
+
+
+def test_runs_are_deterministic():
+    desc = S.cart_desc((40, 33, 20))
+    ic = S.lism_ic(seed=8)
+    out = []
+    for _ in range(2):
+        with S.Solver(desc, ic=ic) as s:
+            s.step(10, S.step_opts())
+            out.append(s.conserved())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_negative_density_is_reported_not_fatal():
+    # a 1e3x oversized first dt drives densities negative: the step returns ENEGDENS, names the
+    # first bad cell, and the handle stays usable (the reference prints and STOPs)
+    desc = S.cart_desc(16, dt_init=0.5)
+    with S.Solver(desc, ic=S.lism_ic()) as s:
+        with pytest.raises(S.SetbError) as e:
+            s.step(1, S.step_opts())
+        assert e.value.code == 4
+        d = s.status()
+        assert d.n_negdens > 0 and 0 <= d.first_bad_cell < 16 ** 3
+        s.set_state(S.fill_lism(desc, S.lism_ic()), 0.0)
+        assert s.status().n_negdens == 0
