@@ -176,6 +176,29 @@ SETB_API int32_t setb_stream(setb_handle* h, void** stream);
 
 SETB_API int32_t setb_destroy(setb_handle* h);
 
+/* No counterpart in the reference.  A variant of setb_step that allocates nothing, for callers
+ * that cannot let a library allocate device memory: hosts that already own the state in their
+ * own device arrays (a CUDA Fortran host's `device` allocatables) or that reserve HBM up front in
+ * their own arena, where a cudaMalloc inside the library could synchronise the device or take
+ * memory promised elsewhere.  The caller passes the conserved state it owns: U is a device
+ * pointer to 8 planes (rho, mx, my, mz, E, Bx, By, Bz), plane v at U + v*var_stride, each plane
+ * nx*ny*nz doubles with x fastest; it is advanced in place by nsteps steps of `o`.  *dt_io is the
+ * dt of the first step on entry (desc->dt_init on a fresh run; desc->dt_init is not used) and the
+ * dt of the next step on return; *time_io is the simulated time in and out; diag may be NULL.
+ * Runs on `stream` (NULL: the legacy default stream) and waits for it before returning.
+ *
+ * The scratch (the Heun stage buffer, the device clock, the error counters) is one fixed
+ * file-scope device array of 16 MiB + 256 B that every GPU loading the library holds until the
+ * process exits.  Limit: var_stride <= 262144 (64^3 cells); larger sizes return SETB_ESIZE.
+ * Every call shares that array and it keeps the last call's contents: the clock and counters are
+ * cleared at the start of each call, and calls that overlap on the GPU (other threads, other
+ * streams) race on it.  The first call on a device resolves the array's device address with
+ * cudaGetSymbolAddress (once per device, with that device current); make that first call before
+ * any stream capture.  No cudaMalloc, cudaFree or other allocating routine is called. */
+SETB_API int32_t setb_step_noalloc(const setb_cart_desc* d, const setb_step_opts* o, double* U,
+                                   int64_t var_stride, int32_t nsteps, double* dt_io, double* time_io,
+                                   setb_diag* diag, void* stream);
+
 SETB_API const char* setb_strerror(int32_t code);
 
 /* Library version, e.g. 100 for 1.0.0. */

@@ -89,6 +89,8 @@ _SIGS = {
     "setb_status": (C.c_int32, [C.c_void_p, C.POINTER(Diag)]),
     "setb_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "setb_destroy": (C.c_int32, [C.c_void_p]),
+    "setb_step_noalloc": (C.c_int32, [C.POINTER(CartDesc), C.POINTER(StepOpts), C.c_void_p, C.c_int64, C.c_int32,
+                                      _dp, _dp, C.POINTER(Diag), C.c_void_p]),
 }
 
 _lib = None
@@ -207,6 +209,18 @@ def chlld_batch(n_state, normals, q1, q2, w=None, n_disc=0, precision=0):
                                 _p(qqq), _p(sp), fl.ctypes.data_as(_ip))
     _check(rc, "setb_chlld_batch")
     return qqq, sp, fl
+
+
+def step_noalloc(desc: CartDesc, opts: StepOpts, U_ptr: int, var_stride: int, nsteps: int, dt: float,
+                 time_all: float, stream: int = 0):
+    """setb_step_noalloc: advance a caller-owned device state (8 planes at var_stride) in place
+    without any allocation by the library.  Returns (dt for the next step, time, Diag)."""
+    dt_c, t_c = C.c_double(dt), C.c_double(time_all)
+    d = Diag()
+    rc = lib().setb_step_noalloc(C.byref(desc), C.byref(opts), C.c_void_p(U_ptr), int(var_stride), int(nsteps),
+                                 C.byref(dt_c), C.byref(t_c), C.byref(d), C.c_void_p(stream or None))
+    _check(rc, "setb_step_noalloc")
+    return dt_c.value, t_c.value, d
 
 
 # ------------------------------------------------------------------------ device-resident solver
