@@ -159,6 +159,11 @@ SETB_API int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_a
  * 1..8, set the simulated time, reset the lagged dt to dt_init and clear the counters. */
 SETB_API int32_t setb_set_state(setb_handle* h, const double* cell_par, double time_all);
 
+/* Copies the resident state, clock and counters of `src` into `dst` on the device (both handles
+ * must describe the same grid); used to restart a solve from a stored initial state without a
+ * host round trip.  Enqueued on dst's stream after waiting for src's. */
+SETB_API int32_t setb_copy_state(setb_handle* dst, setb_handle* src);
+
 /* Device pointers of the conserved state (rho, mx, my, mz, E, Bx, By, Bz), structure of arrays:
  * variable v of cell (i,j,k) is at base[v*var_stride + k*plane_stride + j*row_pitch + i]. */
 SETB_API int32_t setb_state_view(setb_handle* h, double** base, int64_t* var_stride, int64_t* plane_stride,

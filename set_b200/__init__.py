@@ -86,6 +86,7 @@ _SIGS = {
     "setb_state_view": (C.c_int32, [C.c_void_p, C.POINTER(_dp), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
                                     C.POINTER(C.c_int64)]),
     "setb_get_conserved": (C.c_int32, [C.c_void_p, _dp]),
+    "setb_copy_state": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "setb_status": (C.c_int32, [C.c_void_p, C.POINTER(Diag)]),
     "setb_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "setb_destroy": (C.c_int32, [C.c_void_p]),
@@ -303,6 +304,10 @@ class Solver:
         _check(lib().setb_state_view(self.h, C.byref(base), C.byref(vs), C.byref(ps), C.byref(px)),
                "setb_state_view")
         return C.cast(base, C.c_void_p).value, vs.value, ps.value, px.value
+
+    def copy_from(self, other: "Solver"):
+        """Device-side copy of another handle's state, clock and counters (same grid)."""
+        _check(lib().setb_copy_state(self.h, other.h), "setb_copy_state")
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -25,6 +25,8 @@ struct setb_handle {
     GridGeom g{};
     double* buf[2] = {nullptr, nullptr};   // conserved SoA, 8 * vs doubles each
     int cur = 0;                           // buf[cur] holds U^n
+    float* comp = nullptr;                 // mixed form: FP32 compensation, 8 * vs floats
+    bool comp_clean = false;               // comp holds zeros for the current state
     DevClock* clk = nullptr;
     DevStatus* st = nullptr;
     DevClock* h_clk = nullptr;             // pinned mirrors
@@ -59,7 +61,7 @@ int validate_opts(const setb_step_opts* o) {
     if (o->n_disc < 0 || o->n_disc > 2) return SETB_EINVAL;
     if (o->order != 1 && o->order != 2) return SETB_EINVAL;
     if (o->scheme != 1 && o->scheme != 2) return SETB_EINVAL;
-    if (o->precision != 0) return SETB_EINVAL;
+    if (o->precision != 0 && o->precision != 1) return SETB_EINVAL;
     if (o->reserved != 0) return SETB_EINVAL;
     if (!(o->cfl > 0.0)) return SETB_EINVAL;
     return SETB_OK;
@@ -159,6 +161,7 @@ void destroy_impl(setb_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (double* b : h->buf)
         if (b) cudaFree(b);
+    if (h->comp) cudaFree(h->comp);
     if (h->clk) cudaFree(h->clk);
     if (h->st) cudaFree(h->st);
     if (h->h_clk) cudaFreeHost(h->h_clk);
@@ -186,8 +189,7 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
         return SETB_ECUDA;
     }
     h->sm_count = prop.multiProcessorCount;
-    h->ctas_per_sm = std::max(1, (int)(prop.sharedMemPerMultiprocessor / (stage_fp64_smem_bytes() + 2048)));
-    h->ctas_per_sm = std::min(h->ctas_per_sm, 1);   // 256 threads x up to 255 registers
+    h->ctas_per_sm = 1;   // plain form: 256 threads x up to 255 registers; the mixed form runs 2
     h->g.lz = choose_lz(h->g, h->sm_count, h->ctas_per_sm);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
@@ -214,6 +216,7 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
 
 // Uploads Cell_par columns 1..8 (16 doubles per cell) into buf[cur] through buf[1-cur].
 int upload_cellpar(setb_handle* h, const double* cell_par) {
+    h->comp_clean = false;
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
     double* stage = h->buf[1 - h->cur];
     SB_TRY(cudaMemcpy2DAsync(stage, 8 * sizeof(double), cell_par, 16 * sizeof(double), 8 * sizeof(double), N,
@@ -374,6 +377,25 @@ namespace {
 int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaEvent_t* ev) {
     StageArgs a{};
     a.g = h->g;
+    const int P = o->precision;
+    a.g.lz = choose_lz(h->g, h->sm_count, P ? 2 : 1);
+    float* comp = nullptr;
+    if (P == 1) {
+        if (!h->comp) {
+            if (cudaMalloc(&h->comp, sizeof(float) * 8 * (size_t)h->g.vs) != cudaSuccess) {
+                cudaGetLastError();
+                return SETB_ENOMEM;
+            }
+            h->comp_clean = false;
+        }
+        if (!h->comp_clean) {
+            SB_TRY(cudaMemsetAsync(h->comp, 0, sizeof(float) * 8 * (size_t)h->g.vs, h->stream));
+            h->comp_clean = true;
+        }
+        comp = h->comp;
+    } else {
+        h->comp_clean = false;   // plain steps leave the compensation stale
+    }
     a.clk = h->clk;
     a.st = h->st;
     a.cfl = o->cfl;
@@ -387,20 +409,23 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
             a.Ubase = nullptr;
             a.Uout = W;
             a.finalize = 0;
-            SB_TRY(launch_stage_fp64(a, o->n_state, o->order, 0, true, h->stream));
+            a.comp = nullptr;
+            SB_TRY(launch_stage(a, P, o->n_state, o->order, 0, true, h->stream));
             if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
             a.Uin = W;
             a.Ubase = U;
             a.Uout = U;
             a.finalize = 1;
-            SB_TRY(launch_stage_fp64(a, o->n_state, o->order, 1, false, h->stream));
+            a.comp = comp;
+            SB_TRY(launch_stage(a, P, o->n_state, o->order, 1, false, h->stream));
             if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
         } else {
             a.Uin = U;
             a.Ubase = nullptr;
             a.Uout = W;
             a.finalize = 1;
-            SB_TRY(launch_stage_fp64(a, o->n_state, o->order, 0, true, h->stream));
+            a.comp = comp;
+            SB_TRY(launch_stage(a, P, o->n_state, o->order, 0, true, h->stream));
             if (ev) {
                 SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
                 SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
@@ -494,6 +519,20 @@ int32_t setb_set_state(setb_handle* h, const double* cell_par, double time_all) 
     int rc = upload_cellpar(h, cell_par);
     if (rc) return rc;
     return upload_clock(h);
+}
+
+int32_t setb_copy_state(setb_handle* dst, setb_handle* src) {
+    if (!dst || !src) return SETB_EINVAL;
+    if (dst->g.nx != src->g.nx || dst->g.ny != src->g.ny || dst->g.nz != src->g.nz || dst->g.vs != src->g.vs)
+        return SETB_EINVAL;
+    cudaSetDevice(dst->device);
+    SB_TRY(cudaStreamSynchronize(src->stream));
+    SB_TRY(cudaMemcpyAsync(dst->buf[dst->cur], src->buf[src->cur], sizeof(double) * 8 * (size_t)src->g.vs,
+                           cudaMemcpyDeviceToDevice, dst->stream));
+    SB_TRY(cudaMemcpyAsync(dst->clk, src->clk, sizeof(DevClock), cudaMemcpyDeviceToDevice, dst->stream));
+    SB_TRY(cudaMemcpyAsync(dst->st, src->st, sizeof(DevStatus), cudaMemcpyDeviceToDevice, dst->stream));
+    dst->comp_clean = false;
+    return SETB_OK;
 }
 
 int32_t setb_state_view(setb_handle* h, double** base, int64_t* var_stride, int64_t* plane_stride,

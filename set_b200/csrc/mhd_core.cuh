@@ -44,10 +44,14 @@ constexpr double kTtEps = 1.0e-9;                   // Solvers.f90:1625,1634
 enum : int { kFlagWave = 1, kFlagStar = 2 };
 
 // ------------------------------------------------------------------ elementary functions
+// FP64: IEEE square root and correctly rounded reciprocal.  FP32 (the mixed form's Riemann
+// arithmetic): the hardware approximations (MUFU rsqrt / reciprocal, ~2 ulp).
 SB_HD double sb_sqrt(double x) { return sqrt(x); }
 SB_HD float sb_sqrt(float x) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && defined(SB_FP32_IEEE)
     return __fsqrt_rn(x);
+#elif defined(__CUDA_ARCH__)
+    return x > 0.0f ? x * rsqrtf(x) : 0.0f;
 #else
     return std::sqrt(x);
 #endif
@@ -60,8 +64,10 @@ SB_HD double sb_rcp(double x) {
 #endif
 }
 SB_HD float sb_rcp(float x) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && defined(SB_FP32_IEEE)
     return __frcp_rn(x);
+#elif defined(__CUDA_ARCH__)
+    return __fdividef(1.0f, x);
 #else
     return 1.0f / x;
 #endif
@@ -133,21 +139,23 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     const T r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
     const T bx2 = q2[5] * ispi4, by2 = q2[6] * ispi4, bz2 = q2[7] * ispi4;
 
-    // fast magnetosonic speeds, Solvers.f90:1282-1306
+    // fast magnetosonic speeds, Solvers.f90:1282-1306.  The reference forms
+    // cf = (sqrt(b2/r + c(c + 2a)) + sqrt(b2/r + c(c - 2a)))/2 with c = sqrt(ga p/r),
+    // a = bn/sqrt(r); squaring gives the same speed as
+    // cf^2 = (c^2 + b2/r + sqrt((c^2 + b2/r)^2 - 4 c^2 bn^2/r))/2, which needs two square roots
+    // per side instead of three plus a reciprocal square root.
     const T ir1 = sb_rcp(r1), ir2 = sb_rcp(r2);
-    const T aaL = bx1 * sb_rsqrt(r1);
     const T b2L = (bx1 * bx1 + by1 * by1) + bz1 * bz1;
     const T b21 = b2L * ir1;
-    const T cL = sb_sqrt(ga * p1 * ir1);
-    const T cfL = half * (sb_sqrt(sb_pos(b21 + cL * (cL + T(2) * aaL))) +
-                          sb_sqrt(sb_pos(b21 + cL * (cL - T(2) * aaL))));
+    const T c2L = ga * p1 * ir1;
+    const T sL = c2L + b21;
+    const T cfL = sb_sqrt(half * (sL + sb_sqrt(sb_pos(sL * sL - T(4) * c2L * (bx1 * bx1 * ir1)))));
     const T ptL = p1 + half * b2L;
-    const T aaR = bx2 * sb_rsqrt(r2);
     const T b2R = (bx2 * bx2 + by2 * by2) + bz2 * bz2;
     const T b22 = b2R * ir2;
-    const T cR = sb_sqrt(ga * p2 * ir2);
-    const T cfR = half * (sb_sqrt(sb_pos(b22 + cR * (cR + T(2) * aaR))) +
-                          sb_sqrt(sb_pos(b22 + cR * (cR - T(2) * aaR))));
+    const T c2R = ga * p2 * ir2;
+    const T sR = c2R + b22;
+    const T cfR = sb_sqrt(half * (sR + sb_sqrt(sb_pos(sR * sR - T(4) * c2R * (bx2 * bx2 * ir2)))));
     const T ptR = p2 + half * b2R;
 
     // wave-speed estimates, :1308-1330
@@ -155,7 +163,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     T SR = sb_max(u1 + cfL, u2 + cfR);
     T cfC = T(0), vC1 = T(0);
     if (n_disc != 0 || NSTATE == 0) {
-        const T aC = half * (aaL + aaR);
+        const T aC = half * (bx1 * sb_rsqrt(r1) + bx2 * sb_rsqrt(r2));
         const T b2o = half * (b22 + b21);
         const T cC = sb_sqrt(ga * (half * (p2 + p1)) * sb_rcp(half * (r2 + r1)));
         cfC = half * (sb_sqrt(sb_pos(b2o + cC * (cC + T(2) * aC))) +
@@ -245,9 +253,10 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         int region;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
         T vzz2 = T(0), vzz3 = T(0), bzz2 = T(0), bzz3 = T(0), ezzL = T(0), ezzR = T(0);
         T SZL = SM, SZR = SM;
+        T ptz;   // total pressure of the star states
         bool ibn = false;
         if (NSTATE == 2) {   // HLLC, :1465-1567
-            const T ptz = half * ((ptR + r2 * suR * (SM - u2)) + (ptL + r1 * suL * (SM - u1)));
+            ptz = half * ((ptR + r2 * suR * (SM - u2)) + (ptL + r1 * suL * (SM - u1)));
             const T uz0 = ((SR * r2 - SL * r1) + FL[0] - FR[0]) * isrl;
             const T uz1 = ((SR * UR[1] - SL * UL[1]) + FL[1] - FR[1]) * isrl;
             const T uz2 = ((SR * UR[2] - SL * UL[2]) + FL[2] - FR[2]) * isrl;
@@ -275,7 +284,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             else if (SL > wv) region = 1;
             else region = 0;
         } else {             // HLLD, :1598-1814
-            const T ptz = ((suR * r2 * ptL - suL * r1 * ptR) + r1 * r2 * suR * suL * (u2 - u1)) * idd;
+            ptz = ((suR * r2 * ptL - suL * r1 * ptR) + r1 * r2 * suR * suL * (u2 - u1)) * idd;
             const T bn2 = bn * bn;
             T tvR = T(0), tbR = T(0), tvL = T(0), tbL = T(0);
             const T ttR = r2 * suR * (SR - SM) - bn2;
@@ -302,14 +311,15 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             const T sbvR = (bn * SM + bzR2 * vzR2) + bzR3 * vzR3;
             ezR = e2 * suRm + (((ptz * SM - ptR * u2) + bn * (sbv2 - sbvR)) * isrm);
             ezL = e1 * suLm + (((ptz * SM - ptL * u1) + bn * (sbv1 - sbvL)) * islm);
-            const T rzRs = sb_sqrt(rzR), rzLs = sb_sqrt(rzL);
+            const T isR = sb_rsqrt(rzR), isL = sb_rsqrt(rzL);   // 1/sqrt(rho*) and sqrt(rho*) = rho*/sqrt(rho*)
+            const T rzRs = rzR * isR, rzLs = rzL * isL;
             const T abn = sb_abs(bn);
             T sbn = T(0);
             if (abn > T(kEpsB)) {
                 ibn = true;
                 sbn = bn > T(0) ? T(1) : T(-1);
-                SZL = SM - abn * sb_rcp(rzLs);
-                SZR = SM + abn * sb_rcp(rzRs);
+                SZL = SM - abn * isL;
+                SZR = SM + abn * isR;
             }
             const T irzss = sb_rcp(rzRs + rzLs);
             const T rzps = rzRs * rzLs;
@@ -355,11 +365,12 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             if (MOVING) f = f - wv * W[k];
             F[k] = f;
         }
-        if (CHECK_STAR) {
-            const T iw = sb_rcp(W[0]);
-            const T pstar = ((W[4] - half * ((W[1] * W[1] + W[2] * W[2]) + W[3] * W[3]) * iw) -
-                             half * ((W[5] * W[5] + W[6] * W[6]) + W[7] * W[7])) * g1;
-            if (!(W[0] > T(0)) || !(pstar > T(0))) flag |= kFlagStar;
+        if (CHECK_STAR && use1) {
+            // positivity of the selected star state: rho* > 0 and p* = pt* - |b*|^2/2 > 0 (the
+            // gas pressure from the star total pressure avoids the kinetic-energy cancellation
+            // of E - rho|v|^2/2); FL / FR themselves are the reconstructed, positive states
+            const T bb = (bn * bn + W[6] * W[6]) + W[7] * W[7];
+            if (!(rz > T(0)) || !(ptz - half * bb > T(0))) flag |= kFlagStar;
         }
         // normal-field flux, :1570-1581 / :1828-1839
         const T SN = sb_max(sb_abs(SL), sb_abs(SR));

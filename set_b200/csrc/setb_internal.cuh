@@ -47,6 +47,8 @@ struct StageArgs {
     double cfl;
     int n_disc;
     int finalize;                       // last CTA rolls the clock (Euler, or Heun stage 2)
+    float* comp;                        // mixed form: FP32 compensation of the compensated update
+                                        // (Euler / Heun stage 2); null = plain update
 };
 
 // Geometry of cell centres, evaluated with explicitly rounded operations so that host, device
@@ -225,7 +227,13 @@ SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const d
         o[6] = T(q[5] * e2[0] + q[6] * e2[1] + q[7] * e2[2]);
         o[7] = T(q[5] * e3[0] + q[6] * e3[1] + q[7] * e3[2]);
     }
-    const int fl = riemann<T, NSTATE, true, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
+    int fl = riemann<T, NSTATE, true, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
+    if (sizeof(T) == 4 && (fl & kFlagStar)) {
+        // the mixed form's rule: a face whose FP32 star state is not positive is redone in FP64
+        chlld_general<double, NSTATE>(nrm, w, q1d, q2d, n_disc, qqq, sp, flag);
+        *flag |= kFlagStar;
+        return;
+    }
     qqq[0] = F[0];
     qqq[4] = F[4];
     const double nn[3] = {al, be, ge};
@@ -242,6 +250,9 @@ SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const d
 // ---------------------------------------------------------------- launch entry points
 cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int kind, bool want_dt,
                               cudaStream_t s);
+cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
+                         cudaStream_t s);
+int stage_smem_bytes(int precision);
 cudaError_t launch_lism_init(const GridGeom& g, const double* lism, uint64_t seed, double pert,
                              double* U, cudaStream_t s);
 cudaError_t launch_prim_to_cons(const GridGeom& g, const double* prim8, double* U, cudaStream_t s);

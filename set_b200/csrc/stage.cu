@@ -1,0 +1,403 @@
+// stage.cu -- one fused stage of the MHD step on a Cartesian grid, plain FP64 or mixed precision.
+//
+// Replaces the reference's face kernel + cell kernel pair (CUF_MGD_grans_RK2 /
+// CUF_MGD_cell_RK2, SET_Fortran_Cuda_MHD/cuf_solvers.cuf:243-440 and :561-794; Euler variants
+// :62-241, :443-558), which exchange fluxes through a 9 x N_gran array in HBM, with a single
+// kernel per stage:
+//   * a CTA owns a 32 x 8 column of cells and marches along z over lz planes;
+//   * each plane (cells + 2-cell x/y halo) is read from the SoA conserved state once, turned into
+//     primitives once (FP64 pressure recovery) and kept in a 4-plane shared-memory ring
+//     (planes k-1 .. k+2), which is all the z-stencil of the minmod reconstruction needs;
+//   * every face of the plane (x, y and the z face k+1/2) is computed once, by one thread, from
+//     shared memory, and its flux is applied to both neighbouring cells (the z face k-1/2 is
+//     carried in registers from the previous plane);
+//   * the conservative update, p floor, source re-imposition and the dt candidate reduction
+//     (warp shuffle -> one atomicMin per CTA) are fused; the last CTA rolls the lagged-dt clock.
+//
+// P = 0, plain form: everything in FP64.
+// P = 1, mixed form: the ring holds FP32 primitives (recovered from the FP64 state in FP64),
+//   reconstruction and the Riemann solver run in FP32, fluxes are stored in FP32; a face whose
+//   selected FP32 state has rho <= 0 or p <= 0 (or a non-finite flux) is recomputed in FP64 from
+//   the FP64 state; the flux divergence and the update are FP64, and the second Heun stage (or
+//   the Euler step) is a compensated sum with the compensation kept in FP32; dt is reduced in
+//   FP64.  Half the shared memory and at most 128 registers give two CTAs per SM.
+#include <cfloat>
+#include <type_traits>
+#include "setb_internal.cuh"
+
+namespace sb {
+namespace {
+
+// 32 x 8 cells per CTA, one thread per cell.  (288 threads would fit the 808 faces of a plane
+// into three rounds, but a sub-partition holding 3 of 9 warps caps FP64 HLLD at 168 registers
+// and spills.)
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int HX = TX + 4, HY = TY + 4, PLANE = HX * HY;
+constexpr int NZF = NT;                   // z faces k+1/2 of the column tile
+constexpr int NXF = (TX + 1) * TY;        // x faces
+constexpr int NYF = TX * (TY + 1);        // y faces
+constexpr int NF = NZF + NXF + NYF;
+constexpr int RING = 4;
+constexpr int SMEM_ELEMS = RING * 8 * PLANE + 8 * (NZF + NXF + NYF);
+
+__device__ __forceinline__ int ring_slot(int k) { return (k + 4 * RING) & (RING - 1); }
+
+// FP64 primitive state of global cell (i,j,k) with the boundary rules: inflow beyond x = hi,
+// zero-gradient (clamped index) elsewhere.
+__device__ __forceinline__ void fetch_prim64(const StageArgs& A, int i, int j, int k, double* q) {
+    const GridGeom& g = A.g;
+    if (i >= g.nx) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) q[v] = g.inflow[v];
+        return;
+    }
+    i = max(i, 0);
+    j = min(max(j, 0), g.ny - 1);
+    k = min(max(k, 0), g.nz - 1);
+    const long long off = (long long)k * g.ps + (long long)j * g.px + i;
+    double U[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) U[v] = __ldg(A.Uin + v * g.vs + off);
+    double ke, me;
+    prim_from_cons(U, q, ke, me);
+}
+
+// Loads plane kk (with halo) of the tile starting at (i0, j0) as primitives into `dst`.
+template <typename RT>
+__device__ __forceinline__ void load_plane(const StageArgs& A, RT* dst, int i0, int j0, int kk) {
+    for (int c = threadIdx.x; c < PLANE; c += NT) {
+        const int cx = c % HX, cy = c / HX;
+        double q[8];
+        fetch_prim64(A, i0 - 2 + cx, j0 - 2 + cy, kk, q);
+#pragma unroll
+        for (int v = 0; v < 8; v++) dst[v * PLANE + c] = (RT)q[v];
+    }
+}
+
+// The FP64 recompute of one face of the mixed form (rare path; kept out of line so the FP32
+// path keeps its registers).  (i, j, k) is the cell on the high side of the face.
+template <int NSTATE, int ORDER>
+__device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j, int k, double* F, double* sl,
+                                      double* sr) {
+    const int di = axis == 0, dj = axis == 1, dk = axis == 2;
+    double c[4][8];
+    fetch_prim64(A, i - 2 * di, j - 2 * dj, k - 2 * dk, c[0]);
+    fetch_prim64(A, i - di, j - dj, k - dk, c[1]);
+    fetch_prim64(A, i, j, k, c[2]);
+    fetch_prim64(A, i + di, j + dj, k + dk, c[3]);
+    const int pn = 1 + axis, pt1 = axis == 0 ? 2 : 1, pt2 = axis == 2 ? 2 : 3;
+    const int perm[8] = {0, pn, pt1, pt2, 4, 4 + pn, 4 + pt1, 4 + pt2};
+    double f[4][8];
+    for (int s = 0; s < 4; s++)
+        for (int v = 0; v < 8; v++) f[s][v] = c[s][perm[v]];
+    double q1[8], q2[8], G[8], SM;
+    reconstruct<double, ORDER>(f[0], f[1], f[2], f[3], q1, q2);
+    const int fl = riemann<double, NSTATE, false, false>(q1, q2, 0.0, A.n_disc, G, *sl, *sr, SM);
+    for (int v = 0; v < 8; v++) F[perm[v]] = G[v];
+    return fl;
+}
+
+template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
+__global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageArgs A) {
+    using RT = typename std::conditional<P == 0, double, float>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RT* ring = reinterpret_cast<RT*>(smem_raw);
+    RT* fz = ring + RING * 8 * PLANE;   // [8][NZF]
+    RT* fx = fz + 8 * NZF;              // [8][NXF]
+    RT* fy = fx + 8 * NXF;              // [8][NYF]
+    __shared__ double red[NT / 32];
+    __shared__ unsigned long long cnt[5];
+    __shared__ bool last_cta;
+
+    const GridGeom& g = A.g;
+    const int t = threadIdx.x;
+    const int tx = t % TX, ty = t / TX;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+    const int k0 = blockIdx.z * g.lz;
+    const int k1 = min(g.nz, k0 + g.lz);
+    const double dt = A.clk->dt_cur;
+    if (t < 5) cnt[t] = 0;
+
+    double rate = 0.0;   // max over this thread's real faces of max(|SL|,|SR|)/dist
+    unsigned n_recon = 0, n_wave = 0, n_redo = 0;
+
+    // Computes face f of plane k (flattened: z faces, x faces, y faces) into fz/fx/fy.
+    // `dup`: the face is also computed by the CTA below (chunk-boundary z face); it still enters
+    // the dt candidate (min is idempotent) but not the diagnostic counters.
+    auto do_face = [&](int f, int k, bool dup) {
+        int axis, cLL, cL, cR, cRR, fxx, fyy, gk;
+        const RT *sLL, *sL, *sR, *sRR;
+        RT* out;
+        int oidx, ostride;
+        bool real;
+        if (f < NZF) {
+            fxx = f % TX;
+            fyy = f / TX;
+            axis = 2;
+            const int c = (fyy + 2) * HX + fxx + 2;
+            cLL = cL = cR = cRR = c;
+            sLL = ring + ring_slot(k - 1) * 8 * PLANE;
+            sL = ring + ring_slot(k) * 8 * PLANE;
+            sR = ring + ring_slot(k + 1) * 8 * PLANE;
+            sRR = ring + ring_slot(k + 2) * 8 * PLANE;
+            out = fz;
+            oidx = f;
+            ostride = NZF;
+            gk = k + 1;
+            real = (i0 + fxx < g.nx) && (j0 + fyy < g.ny) && (k + 1 <= g.nz) && (k + 1 >= 0);
+        } else if (f < NZF + NXF) {
+            const int idx = f - NZF;
+            fyy = idx / (TX + 1);
+            fxx = idx % (TX + 1);
+            axis = 0;
+            const int c = (fyy + 2) * HX + fxx;   // cell fxx-2 (tile-local) at halo offset +2
+            cLL = c; cL = c + 1; cR = c + 2; cRR = c + 3;
+            sLL = sL = sR = sRR = ring + ring_slot(k) * 8 * PLANE;
+            out = fx;
+            oidx = idx;
+            ostride = NXF;
+            gk = k;
+            real = (i0 + fxx <= g.nx) && (j0 + fyy < g.ny);
+        } else {
+            const int idx = f - NZF - NXF;
+            fyy = idx / TX;
+            fxx = idx % TX;
+            axis = 1;
+            const int c = fyy * HX + fxx + 2;     // row fyy-2 (tile-local)
+            cLL = c; cL = c + HX; cR = c + 2 * HX; cRR = c + 3 * HX;
+            sLL = sL = sR = sRR = ring + ring_slot(k) * 8 * PLANE;
+            out = fy;
+            oidx = idx;
+            ostride = NYF;
+            gk = k;
+            real = (i0 + fxx < g.nx) && (j0 + fyy <= g.ny);
+        }
+        // face-frame permutation of the velocity / B components
+        const int pn = 1 + axis;
+        const int pt1 = axis == 0 ? 2 : 1;
+        const int pt2 = axis == 2 ? 2 : 3;
+        RT qLL[8], qL[8], qR[8], qRR[8];
+        const int perm[8] = {0, pn, pt1, pt2, 4, 4 + pn, 4 + pt1, 4 + pt2};
+#pragma unroll
+        for (int v = 0; v < 8; v++) {
+            const int o = perm[v] * PLANE;
+            qL[v] = sL[o + cL];
+            qR[v] = sR[o + cR];
+            if (v < 5) {
+                qLL[v] = sLL[o + cLL];
+                qRR[v] = sRR[o + cRR];
+            } else {
+                qLL[v] = RT(0);
+                qRR[v] = RT(0);
+            }
+        }
+        RT q1[8], q2[8], F[8], SL, SR, SM;
+        reconstruct<RT, ORDER>(qLL, qL, qR, qRR, q1, q2);
+        if (real && !dup && (q1[0] < RT(0) || q2[0] < RT(0))) n_recon++;
+        int fl = riemann<RT, NSTATE, false, P == 1>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+        double sl = (double)SL, sr = (double)SR;
+        const double sq = g.square[axis];
+        if (P == 1 && real && (fl & kFlagStar)) {
+            double F64[8];
+            fl = face_fp64<NSTATE, ORDER>(A, axis, i0 + fxx, j0 + fyy, gk, F64, &sl, &sr);
+            if (!dup) n_redo++;
+#pragma unroll
+            for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (RT)(F64[v] * sq);
+        } else {
+            if (fl & kFlagWave) {
+#pragma unroll
+                for (int v = 0; v < 8; v++) F[v] = RT(0);
+            }
+#pragma unroll
+            for (int v = 0; v < 8; v++) out[perm[v] * ostride + oidx] = (RT)(F[v] * (RT)sq);
+        }
+        if ((fl & kFlagWave) && real && !dup) n_wave++;
+        if (WANT_DT && real) rate = fmax(rate, fmax(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
+    };
+
+    // ---- prologue: planes k0-2 .. k0+1, then the z face k0-1/2
+    for (int kk = k0 - 2; kk <= k0 + 1; kk++) load_plane<RT>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
+    __syncthreads();
+    double fzl[8];
+    do_face(t, k0 - 1, k0 > 0);   // z face between k0-1 and k0 of column t
+#pragma unroll
+    for (int v = 0; v < 8; v++) fzl[v] = (double)fz[v * NZF + t];
+    __syncthreads();
+
+    const int gi = i0 + tx, gj = j0 + ty;
+    const bool own = (gi < g.nx) && (gj < g.ny);
+    for (int k = k0; k < k1; k++) {
+        load_plane<RT>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
+        __syncthreads();
+        for (int f = t; f < NF; f += NT) do_face(f, k, false);
+        __syncthreads();
+        double fzh[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) fzh[v] = (double)fz[v * NZF + t];
+        if (own) {
+            const long long off = (long long)k * g.ps + (long long)gj * g.px + gi;
+            double un[8], qs[8];
+            bool reset_comp = false;
+            if (source_prim(g, gi, gj, k, qs)) {
+                cons_from_prim_exact(qs, un);
+                reset_comp = true;
+            } else {
+                double uin[8], cmp[8];
+#pragma unroll
+                for (int v = 0; v < 8; v++) {
+                    double pot = 0.0;
+                    pot = pot - (double)fx[v * NXF + ty * (TX + 1) + tx];
+                    pot = pot + (double)fx[v * NXF + ty * (TX + 1) + tx + 1];
+                    pot = pot - (double)fy[v * NYF + ty * TX + tx];
+                    pot = pot + (double)fy[v * NYF + (ty + 1) * TX + tx];
+                    pot = pot - fzl[v];
+                    pot = pot + fzh[v];
+                    uin[v] = A.Uin[v * g.vs + off];
+                    const double inc = dt * (pot * g.inv_vol);
+                    if (P == 1 && A.comp) {
+                        // compensated sum U_new = base + delta (cuf_solvers.cuf:741-770 as an
+                        // increment); the FP32 compensation carries the rounding of the add
+                        const double base = KIND == 0 ? uin[v] : A.Ubase[v * g.vs + off];
+                        const double delta = KIND == 0 ? -inc : 0.5 * ((uin[v] - base) - inc);
+                        const double y = delta - (double)A.comp[v * g.vs + off];
+                        const double s = base + y;
+                        cmp[v] = (s - base) - y;
+                        un[v] = s;
+                    } else if (KIND == 0) {
+                        un[v] = uin[v] - inc;
+                    } else {
+                        un[v] = 0.5 * ((A.Ubase[v * g.vs + off] + uin[v]) - inc);
+                    }
+                }
+                if (!(un[0] > 0.0)) {                    // cuf_solvers.cuf:708-711
+                    atomicAdd(&cnt[0], 1ull);
+                    atomicMin(&A.st->first_bad, (unsigned long long)(gi + (long long)g.nx * (gj + (long long)g.ny * k)));
+#pragma unroll
+                    for (int v = 0; v < 8; v++) un[v] = uin[v];
+                    reset_comp = true;
+                } else {
+                    double q[8], ke, me;
+                    prim_from_cons(un, q, ke, me);
+                    if (q[4] <= 0.0) {                    // cuf_solvers.cuf:777-779
+                        atomicAdd(&cnt[1], 1ull);
+                        un[4] = (kPFloor * kInvG1 + ke) + me;
+                        cmp[4] = 0.0;
+                    }
+                }
+                if (P == 1 && A.comp && !reset_comp) {
+#pragma unroll
+                    for (int v = 0; v < 8; v++) A.comp[v * g.vs + off] = (float)cmp[v];
+                }
+            }
+            if (P == 1 && A.comp && reset_comp) {
+#pragma unroll
+                for (int v = 0; v < 8; v++) A.comp[v * g.vs + off] = 0.0f;
+            }
+#pragma unroll
+            for (int v = 0; v < 8; v++) A.Uout[v * g.vs + off] = un[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 8; v++) fzl[v] = fzh[v];
+    }
+
+    // ---- reductions: counters and the dt candidate
+    if (n_recon) atomicAdd(&cnt[2], (unsigned long long)n_recon);
+    if (n_wave) atomicAdd(&cnt[3], (unsigned long long)n_wave);
+    if (n_redo) atomicAdd(&cnt[4], (unsigned long long)n_redo);
+    if (WANT_DT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
+        if ((t & 31) == 0) red[t >> 5] = rate;
+    }
+    __syncthreads();
+    if (t == 0) {
+        if (WANT_DT) {
+            double r = red[0];
+#pragma unroll
+            for (int w = 1; w < NT / 32; w++) r = fmax(r, red[w]);
+            const double cand = fmin(kDtFaceCap, A.cfl / r);   // r == 0 -> +inf -> cap
+            atomicMin(&A.clk->dt_next, (unsigned long long)__double_as_longlong(cand));
+        }
+        if (cnt[0]) atomicAdd(&A.st->n_negdens, cnt[0]);
+        if (cnt[1]) atomicAdd(&A.st->n_pfloor, cnt[1]);
+        if (cnt[2]) atomicAdd(&A.st->n_recon, cnt[2]);
+        if (cnt[3]) atomicAdd(&A.st->n_wave, cnt[3]);
+        if (cnt[4]) atomicAdd(&A.st->n_redo, cnt[4]);
+        __threadfence();
+        const unsigned total = gridDim.x * gridDim.y * gridDim.z;
+        const unsigned ticket = atomicAdd(&A.clk->counter, 1u);
+        last_cta = (ticket == total - 1);
+    }
+    __syncthreads();
+    if (last_cta && t == 0) {
+        __threadfence();
+        DevClock* c = A.clk;
+        c->counter = 0;
+        if (A.finalize) {
+            const unsigned long long nb = atomicExch(&c->dt_next, (unsigned long long)__double_as_longlong(kDtReset));
+            c->time_all += c->dt_cur;
+            c->dt_last = c->dt_cur;
+            c->dt_cur = __longlong_as_double((long long)nb);
+            c->steps += 1;
+        }
+        __threadfence();
+    }
+}
+
+template <int P>
+constexpr int smem_bytes() {
+    return SMEM_ELEMS * (P == 0 ? (int)sizeof(double) : (int)sizeof(float));
+}
+
+template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
+cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
+    auto kern = stage_kernel<P, NSTATE, ORDER, KIND, WANT_DT>;
+    const int smem = smem_bytes<P>();
+    static bool attr_set = false;   // per process; every device shares the same limit
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, (a.g.nz + a.g.lz - 1) / a.g.lz);
+    kern<<<grid, NT, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P, int NSTATE>
+cudaError_t launch_n(const StageArgs& a, int order, int kind, bool want_dt, cudaStream_t s) {
+    if (order == 2) {
+        if (kind == 0) return want_dt ? launch_t<P, NSTATE, 2, 0, true>(a, s) : launch_t<P, NSTATE, 2, 0, false>(a, s);
+        return launch_t<P, NSTATE, 2, 1, false>(a, s);
+    }
+    if (kind == 0) return want_dt ? launch_t<P, NSTATE, 1, 0, true>(a, s) : launch_t<P, NSTATE, 1, 0, false>(a, s);
+    return launch_t<P, NSTATE, 1, 1, false>(a, s);
+}
+
+template <int P>
+cudaError_t launch_p(const StageArgs& a, int n_state, int order, int kind, bool want_dt, cudaStream_t s) {
+    switch (n_state) {
+        case 0: return launch_n<P, 0>(a, order, kind, want_dt, s);
+        case 1: return launch_n<P, 1>(a, order, kind, want_dt, s);
+        case 2: return launch_n<P, 2>(a, order, kind, want_dt, s);
+        default: return launch_n<P, 3>(a, order, kind, want_dt, s);
+    }
+}
+
+}  // namespace
+
+int stage_smem_bytes(int precision) { return precision ? smem_bytes<1>() : smem_bytes<0>(); }
+int stage_fp64_smem_bytes() { return smem_bytes<0>(); }
+
+cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
+                         cudaStream_t s) {
+    return precision ? launch_p<1>(a, n_state, order, kind, want_dt, s)
+                     : launch_p<0>(a, n_state, order, kind, want_dt, s);
+}
+
+cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int kind, bool want_dt,
+                              cudaStream_t s) {
+    return launch_p<0>(a, n_state, order, kind, want_dt, s);
+}
+
+}  // namespace sb

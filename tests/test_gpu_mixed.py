@@ -1,0 +1,101 @@
+"""The mixed-precision form against FP64.
+
+Mixed form: FP32 reconstruction and Riemann arithmetic, FP64 state, FP64 pressure recovery, FP64
+dt reduction, compensated FP64 update, FP64 recompute of faces whose FP32 star state is not
+positive.  Tolerances (stated against FP64 runs of the same problem):
+  * one step from identical input (dt at the CFL limit): per-cell relative error of rho and
+    E <= 1e-6;
+  * 100 steps at 48^3: relative L1 error of rho <= 1e-6 at Mach 2 / beta 10 (measured 2.5e-7) and
+    <= 2e-6 at Mach 8 / beta 0.1 (measured 9.7e-7: the FP32 rounding of O(|F|) flux values,
+    amplified ~60x into the pressure when E is dominated by kinetic and magnetic energy); p and
+    |B| <= 1e-5; relative drift of the total energy between the two runs <= 1e-6.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import set_b200 as S
+from tests.test_gpu_parity import oracle_opts, oracle_problem
+
+pytestmark = pytest.mark.gpu
+
+
+def prim_fields(U):
+    rho = U[0]
+    m = U[1:4]
+    B = U[5:8]
+    ke = 0.5 * (m ** 2).sum(0) / rho
+    me = 0.5 * (B ** 2).sum(0) / (4 * np.pi)
+    p = (U[4] - ke - me) * (5.0 / 3.0 - 1.0)
+    return rho, p, np.sqrt((B ** 2).sum(0))
+
+
+def rel_l1(a, b):
+    return np.abs(a - b).sum() / np.abs(b).sum()
+
+
+@pytest.mark.parametrize("shape,n_state,scheme", [((40, 24, 36), 3, 2), ((24, 20, 18), 2, 2), ((20, 16, 12), 3, 1)])
+def test_mixed_one_step_close_to_oracle(shape, n_state, scheme):
+    inflow = S.lism_prim(bmag=0.0 if n_state == 2 else 1.0)
+    desc = S.cart_desc(shape, inflow=inflow, dt_init=5e-4)
+    ic = S.lism_ic(lism=inflow, seed=21)
+    o = S.step_opts(n_state=n_state, order=2 if scheme == 2 else 1, scheme=scheme, precision=1)
+    g, Uo = oracle_problem(desc, ic)
+    O.run(g, oracle_opts(o), Uo, 1)
+    with S.Solver(desc, ic=ic) as s:
+        s.step(1, o)
+        Ug = s.conserved()
+    for v in (0, 4):
+        assert (np.abs(Ug[v] - Uo[v]) / np.abs(Uo[v])).max() <= 1e-6
+
+
+@pytest.mark.parametrize("mach,beta", [(2.0, 10.0), (8.0, 0.1)])
+def test_mixed_100_steps_l1_vs_fp64(mach, beta):
+    # LISM inflow at Mach `mach` and plasma beta `beta` (config C3's range), 48^3, 100 steps
+    rho, p = 1.0, 1.0
+    c = np.sqrt(5.0 / 3.0 * p / rho)
+    bmag = np.sqrt(2.0 * p / beta) * np.sqrt(4 * np.pi)   # beta = 2p/|b|^2, b = B/sqrt(4pi)
+    inflow = S.lism_prim(rho=rho, p=p, u=(-mach * c, 0.0, 0.0), bmag=bmag, tilt_deg=60.0)
+    desc = S.cart_desc(48, inflow=inflow)
+    ic = S.lism_ic(lism=inflow, seed=31)
+    res = {}
+    for prec in (0, 1):
+        with S.Solver(desc, ic=ic) as s:
+            s.step(100, S.step_opts(precision=prec))
+            res[prec] = (s.conserved(), s.status())
+    U64, U32 = res[0][0], res[1][0]
+    r64, p64, b64 = prim_fields(U64)
+    r32, p32, b32 = prim_fields(U32)
+    e_rho, e_p, e_b = rel_l1(r32, r64), rel_l1(p32, p64), rel_l1(b32, b64)
+    drift = abs(U32[4].sum() - U64[4].sum()) / abs(U64[4].sum())
+    print(f"mach {mach} beta {beta}: L1 rho {e_rho:.2e} p {e_p:.2e} |B| {e_b:.2e} energy drift {drift:.2e} "
+          f"fp64 redo {res[1][1].n_fp64_redo}")
+    assert e_rho <= (1e-6 if mach < 4 else 2e-6)
+    assert e_p <= 1e-5 and e_b <= 1e-5
+    assert drift <= 1e-6
+    assert res[1][1].n_negdens == 0
+
+
+def test_mixed_switching_precision_resets_compensation():
+    # plain -> mixed -> plain on one handle stays close to an all-plain run
+    desc = S.cart_desc((32, 24, 20))
+    ic = S.lism_ic(seed=41)
+    with S.Solver(desc, ic=ic) as a, S.Solver(desc, ic=ic) as b:
+        a.step(30, S.step_opts(precision=0))
+        b.step(10, S.step_opts(precision=0))
+        b.step(10, S.step_opts(precision=1))
+        b.step(10, S.step_opts(precision=0))
+        ra, _, _ = prim_fields(a.conserved())
+        rb, _, _ = prim_fields(b.conserved())
+    assert rel_l1(rb, ra) <= 1e-6
+
+
+def test_mixed_is_deterministic():
+    desc = S.cart_desc((40, 33, 20))
+    ic = S.lism_ic(seed=8)
+    out = []
+    for _ in range(2):
+        with S.Solver(desc, ic=ic) as s:
+            s.step(10, S.step_opts(precision=1))
+            out.append(s.conserved())
+    np.testing.assert_array_equal(out[0], out[1])
