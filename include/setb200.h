@@ -181,6 +181,38 @@ SETB_API int32_t setb_stream(setb_handle* h, void** stream);
 
 SETB_API int32_t setb_destroy(setb_handle* h);
 
+/* ------------------------------------------------------------------ batched solves
+ * No counterpart in the reference (one grid per process, cuf_kernel.cuf:351-382).  A batch
+ * advances many Cartesian solves of uneven size together: every step is two persistent launches
+ * whose CTAs draw 32x8xlz tiles of all active solves from one work queue; each solve keeps its own
+ * lagged dt and clock, so a solve's results do not depend on what else is in the batch.  Solves
+ * are admitted by HBM footprint and can be added or removed between steps (continuous batching).
+ * Supported per solve: n_state 2 (HLLC) or 3 (HLLD), order 2, scheme 2, the batch's precision. */
+typedef struct setb_batch setb_batch;
+
+SETB_API int32_t setb_batch_create(setb_batch** b, int32_t max_slots, int32_t precision, int64_t hbm_budget_bytes);
+/* Admits one solve (seeded initial condition generated on the device); SETB_EBUSY when no slot
+ * is free or its footprint would exceed the budget. */
+SETB_API int32_t setb_batch_add(setb_batch* b, const setb_cart_desc* d, const setb_lism_ic* ic,
+                                const setb_step_opts* o, int32_t* slot);
+SETB_API int32_t setb_batch_remove(setb_batch* b, int32_t slot);
+/* Advances every active solve by nsteps (asynchronous; chunks of steps replay a CUDA graph). */
+SETB_API int32_t setb_batch_step(setb_batch* b, int32_t nsteps);
+/* Steady-state check: rel_change[slot] = sum|rho - rho_prev| / sum|rho| since the previous check
+ * of that solve (fixed-order, deterministic reduction), -1 on a solve's first check or for free
+ * slots; then rho_prev = rho.  rel_change has max_slots entries.  Waits for the batch. */
+SETB_API int32_t setb_batch_check(setb_batch* b, double* rel_change);
+SETB_API int32_t setb_batch_get_conserved(setb_batch* b, int32_t slot, double* U);
+SETB_API int32_t setb_batch_status(setb_batch* b, int32_t slot, setb_diag* out);
+SETB_API int32_t setb_batch_info(setb_batch* b, int64_t* bytes_used, int32_t* active, int32_t* lz, int32_t* grid);
+/* Tiling of the batch launches: z-march length lz and persistent CTAs per SM slot multiplier. */
+SETB_API int32_t setb_batch_set_tiling(setb_batch* b, int32_t lz, int32_t grid_mult);
+/* Autotuner: times `reps` first-stage launches (idempotent on the state) for each candidate
+ * tiling on the current membership, keeps the fastest. */
+SETB_API int32_t setb_batch_tune(setb_batch* b, int32_t reps, int32_t* lz, int32_t* grid_mult, double* ms);
+SETB_API int32_t setb_batch_sync(setb_batch* b);
+SETB_API int32_t setb_batch_destroy(setb_batch* b);
+
 /* No counterpart in the reference.  A variant of setb_step that allocates nothing, for callers
  * that cannot let a library allocate device memory: hosts that already own the state in their
  * own device arrays (a CUDA Fortran host's `device` allocatables) or that reserve HBM up front in

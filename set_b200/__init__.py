@@ -92,6 +92,18 @@ _SIGS = {
     "setb_destroy": (C.c_int32, [C.c_void_p]),
     "setb_step_noalloc": (C.c_int32, [C.POINTER(CartDesc), C.POINTER(StepOpts), C.c_void_p, C.c_int64, C.c_int32,
                                       _dp, _dp, C.POINTER(Diag), C.c_void_p]),
+    "setb_batch_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int64]),
+    "setb_batch_add": (C.c_int32, [C.c_void_p, C.POINTER(CartDesc), C.POINTER(LismIC), C.POINTER(StepOpts), _ip]),
+    "setb_batch_remove": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "setb_batch_step": (C.c_int32, [C.c_void_p, C.c_int32]),
+    "setb_batch_check": (C.c_int32, [C.c_void_p, _dp]),
+    "setb_batch_get_conserved": (C.c_int32, [C.c_void_p, C.c_int32, _dp]),
+    "setb_batch_status": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(Diag)]),
+    "setb_batch_info": (C.c_int32, [C.c_void_p, C.POINTER(C.c_int64), _ip, _ip, _ip]),
+    "setb_batch_set_tiling": (C.c_int32, [C.c_void_p, C.c_int32, C.c_int32]),
+    "setb_batch_tune": (C.c_int32, [C.c_void_p, C.c_int32, _ip, _ip, _dp]),
+    "setb_batch_sync": (C.c_int32, [C.c_void_p]),
+    "setb_batch_destroy": (C.c_int32, [C.c_void_p]),
 }
 
 _lib = None
@@ -328,3 +340,93 @@ class Problem:
     ic: LismIC
     opts: StepOpts
     steps: int
+
+
+class Batch:
+    """Many Cartesian solves advanced together (setb_batch_*): admission by HBM footprint,
+    add/remove between steps, per-solve lagged dt."""
+
+    def __init__(self, max_slots: int, precision: int = 1, hbm_budget: int = 150 * 10 ** 9):
+        h = C.c_void_p()
+        _check(lib().setb_batch_create(C.byref(h), int(max_slots), int(precision), int(hbm_budget)),
+               "setb_batch_create")
+        self.h = h
+        self.max_slots = max_slots
+        self.precision = precision
+        self.shapes = {}
+
+    def close(self):
+        if self.h:
+            lib().setb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def add(self, desc: CartDesc, ic: LismIC, opts: StepOpts) -> int:
+        """Admit a solve; returns its slot, or raises SetbError(EBUSY=11) when it does not fit."""
+        slot = C.c_int32()
+        _check(lib().setb_batch_add(self.h, C.byref(desc), C.byref(ic), C.byref(opts), C.byref(slot)),
+               "setb_batch_add")
+        self.shapes[slot.value] = (desc.nz, desc.ny, desc.nx)
+        return slot.value
+
+    def try_add(self, desc: CartDesc, ic: LismIC, opts: StepOpts):
+        """Admit a solve; None when it does not fit (budget or slots)."""
+        slot = C.c_int32()
+        rc = lib().setb_batch_add(self.h, C.byref(desc), C.byref(ic), C.byref(opts), C.byref(slot))
+        if rc == 11:
+            return None
+        _check(rc, "setb_batch_add")
+        self.shapes[slot.value] = (desc.nz, desc.ny, desc.nx)
+        return slot.value
+
+    def remove(self, slot: int):
+        _check(lib().setb_batch_remove(self.h, int(slot)), "setb_batch_remove")
+        self.shapes.pop(slot, None)
+
+    def step(self, nsteps: int):
+        _check(lib().setb_batch_step(self.h, int(nsteps)), "setb_batch_step")
+
+    def sync(self):
+        _check(lib().setb_batch_sync(self.h), "setb_batch_sync")
+
+    def check(self) -> np.ndarray:
+        out = np.zeros(self.max_slots)
+        _check(lib().setb_batch_check(self.h, _p(out)), "setb_batch_check")
+        return out
+
+    def conserved(self, slot: int) -> np.ndarray:
+        U = np.zeros((8,) + self.shapes[slot])
+        _check(lib().setb_batch_get_conserved(self.h, int(slot), _p(U)), "setb_batch_get_conserved")
+        return U
+
+    def status(self, slot: int, check: bool = True) -> Diag:
+        d = Diag()
+        rc = lib().setb_batch_status(self.h, int(slot), C.byref(d))
+        if check:
+            _check(rc, "setb_batch_status")
+        return d
+
+    def info(self):
+        used, act, lz, grid = C.c_int64(), C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().setb_batch_info(self.h, C.byref(used), C.byref(act), C.byref(lz), C.byref(grid)),
+               "setb_batch_info")
+        return {"bytes_used": used.value, "active": act.value, "lz": lz.value, "grid": grid.value}
+
+    def set_tiling(self, lz: int, grid_mult: int = 1):
+        _check(lib().setb_batch_set_tiling(self.h, int(lz), int(grid_mult)), "setb_batch_set_tiling")
+
+    def tune(self, reps: int = 3):
+        lz, gm, ms = C.c_int32(), C.c_int32(), C.c_double()
+        _check(lib().setb_batch_tune(self.h, int(reps), C.byref(lz), C.byref(gm), C.byref(ms)), "setb_batch_tune")
+        return {"lz": lz.value, "grid_mult": gm.value, "ms_per_stage1": ms.value}

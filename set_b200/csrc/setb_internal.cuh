@@ -49,6 +49,16 @@ struct StageArgs {
     int finalize;                       // last CTA rolls the clock (Euler, or Heun stage 2)
     float* comp;                        // mixed form: FP32 compensation of the compensated update
                                         // (Euler / Heun stage 2); null = plain update
+    unsigned total_tiles;               // batch: tiles of this solve in the launch
+    int n_state;                        // batch: per-solve Riemann solver (2 HLLC, 3 HLLD)
+};
+
+// One launch of the batch kernel: tiles of many solves behind one work-queue counter.
+struct BatchArgs {
+    const StageArgs* inst;              // per-slot arguments of this stage (device array)
+    const int4* items;                  // work list: (slot, bx, by, bz), largest solves first
+    int n_items;
+    unsigned* queue;                    // next item to hand out (zeroed before the launch)
 };
 
 // Geometry of cell centres, evaluated with explicitly rounded operations so that host, device
@@ -253,6 +263,10 @@ cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int ki
 cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
                          cudaStream_t s);
 int stage_smem_bytes(int precision);
+cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
+                               cudaStream_t s);
+cudaError_t prepare_batch_kernels(int precision);
+int batch_ctas_per_sm(int precision);
 cudaError_t launch_lism_init(const GridGeom& g, const double* lism, uint64_t seed, double pert,
                              double* U, cudaStream_t s);
 cudaError_t launch_prim_to_cons(const GridGeom& g, const double* prim8, double* U, cudaStream_t s);

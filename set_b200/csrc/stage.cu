@@ -97,8 +97,13 @@ __device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j
     return fl;
 }
 
+// One tile of one stage: the column (bx, by) of 32 x 8 cells, planes [bz*lz, min(nz, (bz+1)*lz)).
+// `total_tiles` is the number of tiles of this solve in the launch; the last one to finish rolls
+// the solve's clock.  Called by the single-solve kernel (one tile per CTA) and by the batch
+// kernel (tiles of many solves drawn from a work queue); every CTA-wide barrier is reached by all
+// threads, and the function ends with one so a CTA may run the next tile immediately.
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageArgs A) {
+__device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int bz, unsigned total_tiles) {
     using RT = typename std::conditional<P == 0, double, float>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RT* ring = reinterpret_cast<RT*>(smem_raw);
@@ -112,8 +117,8 @@ __global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageAr
     const GridGeom& g = A.g;
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
-    const int k0 = blockIdx.z * g.lz;
+    const int i0 = bx * TX, j0 = by * TY;
+    const int k0 = bz * g.lz;
     const int k1 = min(g.nz, k0 + g.lz);
     const double dt = A.clk->dt_cur;
     if (t < 5) cnt[t] = 0;
@@ -215,25 +220,28 @@ __global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageAr
         if (WANT_DT && real) rate = fmax(rate, fmax(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
     };
 
-    // ---- prologue: planes k0-2 .. k0+1, then the z face k0-1/2
-    for (int kk = k0 - 2; kk <= k0 + 1; kk++) load_plane<RT>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
-    __syncthreads();
+    // ---- the march.  Iteration k0-1 is the prologue: planes k0-2 .. k0+1 and only the z face
+    // k0-1/2 (carried into the first update).  Every face goes through the one do_face call
+    // site below, so a face's arithmetic does not depend on where a chunk starts.
+    for (int kk = k0 - 2; kk <= k0; kk++) load_plane<RT>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
     double fzl[8];
-    do_face(t, k0 - 1, k0 > 0);   // z face between k0-1 and k0 of column t
-#pragma unroll
-    for (int v = 0; v < 8; v++) fzl[v] = (double)fz[v * NZF + t];
-    __syncthreads();
-
     const int gi = i0 + tx, gj = j0 + ty;
     const bool own = (gi < g.nx) && (gj < g.ny);
-    for (int k = k0; k < k1; k++) {
+    for (int k = k0 - 1; k < k1; k++) {
         load_plane<RT>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
         __syncthreads();
-        for (int f = t; f < NF; f += NT) do_face(f, k, false);
+        const bool pro = (k < k0);
+        const int nf = pro ? NZF : NF;
+        for (int f = t; f < nf; f += NT) do_face(f, k, pro && k0 > 0);
         __syncthreads();
         double fzh[8];
 #pragma unroll
         for (int v = 0; v < 8; v++) fzh[v] = (double)fz[v * NZF + t];
+        if (pro) {
+#pragma unroll
+            for (int v = 0; v < 8; v++) fzl[v] = fzh[v];
+            continue;
+        }
         if (own) {
             const long long off = (long long)k * g.ps + (long long)gj * g.px + gi;
             double un[8], qs[8];
@@ -324,9 +332,8 @@ __global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageAr
         if (cnt[3]) atomicAdd(&A.st->n_wave, cnt[3]);
         if (cnt[4]) atomicAdd(&A.st->n_redo, cnt[4]);
         __threadfence();
-        const unsigned total = gridDim.x * gridDim.y * gridDim.z;
         const unsigned ticket = atomicAdd(&A.clk->counter, 1u);
-        last_cta = (ticket == total - 1);
+        last_cta = (ticket == total_tiles - 1);
     }
     __syncthreads();
     if (last_cta && t == 0) {
@@ -341,6 +348,41 @@ __global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageAr
             c->steps += 1;
         }
         __threadfence();
+    }
+    __syncthreads();
+}
+
+template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
+__global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageArgs A) {
+    run_tile<P, NSTATE, ORDER, KIND, WANT_DT>(A, blockIdx.x, blockIdx.y, blockIdx.z,
+                                               gridDim.x * gridDim.y * gridDim.z);
+}
+
+// Persistent batch kernel: each CTA takes tiles from the work queue until it is empty; the
+// tile's solve selects the arguments (copied to shared memory) and the Riemann solver.  The
+// items of one solve are counted by its own clock, so every solve keeps its own lagged dt.
+template <int P, int ORDER, int KIND, bool WANT_DT>
+__global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) batch_stage_kernel(const BatchArgs B) {
+    __shared__ __align__(16) StageArgs As;
+    __shared__ int4 it;
+    constexpr int WORDS = sizeof(StageArgs) / sizeof(unsigned long long);
+    static_assert(sizeof(StageArgs) % sizeof(unsigned long long) == 0, "StageArgs must be 8-byte granular");
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned i = atomicAdd(B.queue, 1u);
+            it = i < (unsigned)B.n_items ? B.items[i] : make_int4(-1, 0, 0, 0);
+        }
+        __syncthreads();
+        const int4 w = it;
+        if (w.x < 0) break;
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(B.inst + w.x);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&As);
+        for (int q = threadIdx.x; q < WORDS; q += NT) dst[q] = src[q];
+        __syncthreads();
+        if (As.n_state == 3)
+            run_tile<P, 3, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles);
+        else
+            run_tile<P, 2, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles);
     }
 }
 
@@ -384,7 +426,37 @@ cudaError_t launch_p(const StageArgs& a, int n_state, int order, int kind, bool 
     }
 }
 
+template <int P, int KIND, bool WANT_DT>
+cudaError_t batch_attr() {
+    return cudaFuncSetAttribute(batch_stage_kernel<P, 2, KIND, WANT_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_bytes<P>());
+}
+
 }  // namespace
+
+cudaError_t prepare_batch_kernels(int precision) {
+    cudaError_t e;
+    if (precision) {
+        if ((e = batch_attr<1, 0, true>()) != cudaSuccess) return e;
+        return batch_attr<1, 1, false>();
+    }
+    if ((e = batch_attr<0, 0, true>()) != cudaSuccess) return e;
+    return batch_attr<0, 1, false>();
+}
+
+int batch_ctas_per_sm(int precision) { return precision ? 2 : 1; }
+
+cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
+                               cudaStream_t s) {
+    if (precision) {
+        if (kind == 0 && want_dt) batch_stage_kernel<1, 2, 0, true><<<grid, NT, smem_bytes<1>(), s>>>(b);
+        else batch_stage_kernel<1, 2, 1, false><<<grid, NT, smem_bytes<1>(), s>>>(b);
+    } else {
+        if (kind == 0 && want_dt) batch_stage_kernel<0, 2, 0, true><<<grid, NT, smem_bytes<0>(), s>>>(b);
+        else batch_stage_kernel<0, 2, 1, false><<<grid, NT, smem_bytes<0>(), s>>>(b);
+    }
+    return cudaGetLastError();
+}
 
 int stage_smem_bytes(int precision) { return precision ? smem_bytes<1>() : smem_bytes<0>(); }
 int stage_fp64_smem_bytes() { return smem_bytes<0>(); }
