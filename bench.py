@@ -290,6 +290,43 @@ def run_ours(args, world, rank, local):
     e2e = world * cells * T * args.steps / (e2e_ms / 1e3)
     finite = bool(np.isfinite(cp[:, :8]).all())
 
+    # ---- config C4: the 64-grid ensemble (mixed, one batch) vs sequential plain-form solves
+    ensemble = None
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        from set_b200 import workloads as WL
+        inst = WL.c4_instances()
+        small = sorted(range(len(inst)), key=lambda k: inst[k].cells)[:4]
+        bat = WL.run_batched(inst, tune=True, keep=small)
+        seq = WL.run_sequential(inst, precision=0, keep=small)
+        l1 = max(float(np.abs(bat["states"][k][0] - seq["states"][k][0]).sum() / np.abs(seq["states"][k][0]).sum())
+                 for k in small)
+        ensemble = {"config": "C4: 64 grids, edges log-uniform [48,160] per axis, HLLD RK2 minmod mixed, "
+                              "300 steps, CFL 0.2",
+                    "solves_per_s": bat["solves_per_s"], "seconds": bat["seconds"],
+                    "cell_updates_per_s": bat["cell_updates_per_s"], "tuned": bat["tuned"],
+                    "sequential_plain_solves_per_s": seq["solves_per_s"], "sequential_plain_seconds": seq["seconds"],
+                    "speedup_vs_sequential_plain": bat["solves_per_s"] / seq["solves_per_s"],
+                    "l1_rho_vs_plain_max_of_4_smallest": l1, "total_cells": sum(i.cells for i in inst),
+                    "fp64_face_recomputes": bat["fp64_redo"], "n_negdens": bat["n_negdens"],
+                    "n_negdens_sequential": seq["n_negdens"]}
+
+    # ---- config C5 (scaled): a Poisson request stream through the solve server
+    served = None
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        from set_b200 import workloads as WL, serve as SV
+        reqs = WL.c5_requests(count=args.serve_requests, rate=20.0, lo=32, hi=args.serve_max_edge,
+                              max_steps=args.serve_max_steps)
+        out = SV.run_stream(reqs, max_slots=256, precision=1)
+        seq = SV.run_sequential(reqs, precision=0)
+        served = {"config": f"C5 scaled: {len(reqs)} requests, Poisson 20/s, cubic edge log-uniform "
+                            f"[32,{args.serve_max_edge}], 30% hydro (HLLC) / 70% MHD (HLLD), steady state 1e-5 "
+                            f"per 50-step check or cap {args.serve_max_steps} steps, CFL 0.2, 150 GB budget",
+                  "latency_p50_s": out["latency_p50_s"], "latency_p99_s": out["latency_p99_s"],
+                  "solves_per_s": out["solves_per_s"], "span_s": out["span_s"], "max_active": out["max_active"],
+                  "converged": out["converged"], "failed": out["failed"],
+                  "sequential_plain_solves_per_s": seq["solves_per_s"],
+                  "speedup_vs_sequential_plain": out["solves_per_s"] / seq["solves_per_s"]}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, thr, secs = cpu_baseline(n)
@@ -311,6 +348,8 @@ def run_ours(args, world, rank, local):
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
                          "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2}},
             "mixed": mixed,
+            "ensemble": ensemble,
+            "served": served,
             "cpu_baseline": base,
             "clocks": clocks,
             "gpu_launches": int(sum(k_n)),
@@ -333,6 +372,10 @@ def main():
     ap.add_argument("--tsteps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--serve-max-edge", type=int, default=96)
+    ap.add_argument("--serve-max-steps", type=int, default=600)
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

@@ -213,6 +213,47 @@ SETB_API int32_t setb_batch_tune(setb_batch* b, int32_t reps, int32_t* lz, int32
 SETB_API int32_t setb_batch_sync(setb_batch* b);
 SETB_API int32_t setb_batch_destroy(setb_batch* b);
 
+/* ------------------------------------------------------------------ solve server
+ * No counterpart in the reference.  Continuous batching on one GPU: a server thread owns a batch;
+ * requests submitted from any thread are admitted in arrival order, between chunks of
+ * `check_every` steps, while their HBM footprint fits the budget; every chunk advances all
+ * admitted solves together, runs the steady-state check and retires the solves that reached
+ * steady_tol or max_steps.  Destroying the server finishes the admitted and queued solves. */
+typedef struct setb_server setb_server;
+
+typedef struct {
+    setb_cart_desc desc;
+    setb_lism_ic ic;
+    setb_step_opts opts;    /* n_state 2 or 3, order 2, scheme 2, the server's precision     */
+    int32_t max_steps;      /* step cap, applied at chunk granularity                          */
+    int32_t reserved;
+    double steady_tol;      /* stop when sum|rho - rho_prev|/sum|rho| between checks < tol (0: off) */
+    double* result_U;       /* optional host buffer of 8*N doubles for the final conserved state */
+} setb_request;
+
+typedef struct {
+    int64_t id;
+    int32_t status;         /* SETB_OK, or the error that ended the solve                       */
+    int32_t steps;
+    int32_t converged;      /* 1 when stopped by steady_tol                                     */
+    int32_t reserved;
+    double last_change;
+    double time_all;
+    double t_submit, t_admit, t_done;   /* seconds on the server's steady clock                 */
+    setb_diag diag;
+} setb_result;
+
+SETB_API int32_t setb_server_create(setb_server** s, int32_t max_slots, int32_t precision, int64_t hbm_budget,
+                                    int32_t check_every);
+SETB_API int32_t setb_server_submit(setb_server* s, const setb_request* r, int64_t* id);
+/* Waits up to timeout_s seconds for request `id`; SETB_ETIMEOUT when it is not done. */
+SETB_API int32_t setb_server_wait(setb_server* s, int64_t id, setb_result* out, double timeout_s);
+/* Results in completion order not yet polled (at most max). */
+SETB_API int32_t setb_server_poll(setb_server* s, setb_result* out, int32_t max, int32_t* n);
+SETB_API int32_t setb_server_stats(setb_server* s, int32_t* pending, int32_t* active, int64_t* completed,
+                                   int64_t* failed, int32_t* max_active);
+SETB_API int32_t setb_server_destroy(setb_server* s);
+
 /* No counterpart in the reference.  A variant of setb_step that allocates nothing, for callers
  * that cannot let a library allocate device memory: hosts that already own the state in their
  * own device arrays (a CUDA Fortran host's `device` allocatables) or that reserve HBM up front in

@@ -68,6 +68,17 @@ class Diag(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Request(C.Structure):
+    _fields_ = [("desc", CartDesc), ("ic", LismIC), ("opts", StepOpts), ("max_steps", C.c_int32),
+                ("reserved", C.c_int32), ("steady_tol", C.c_double), ("result_U", _dp)]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_int64), ("status", C.c_int32), ("steps", C.c_int32), ("converged", C.c_int32),
+                ("reserved", C.c_int32), ("last_change", C.c_double), ("time_all", C.c_double),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double), ("diag", Diag)]
+
+
 # Every entry point of include/setb200.h: name -> (restype, argtypes)
 _SIGS = {
     "setb_version": (C.c_int32, []),
@@ -104,6 +115,12 @@ _SIGS = {
     "setb_batch_tune": (C.c_int32, [C.c_void_p, C.c_int32, _ip, _ip, _dp]),
     "setb_batch_sync": (C.c_int32, [C.c_void_p]),
     "setb_batch_destroy": (C.c_int32, [C.c_void_p]),
+    "setb_server_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int64, C.c_int32]),
+    "setb_server_submit": (C.c_int32, [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_int64)]),
+    "setb_server_wait": (C.c_int32, [C.c_void_p, C.c_int64, C.POINTER(Result), C.c_double]),
+    "setb_server_poll": (C.c_int32, [C.c_void_p, C.POINTER(Result), C.c_int32, _ip]),
+    "setb_server_stats": (C.c_int32, [C.c_void_p, _ip, _ip, C.POINTER(C.c_int64), C.POINTER(C.c_int64), _ip]),
+    "setb_server_destroy": (C.c_int32, [C.c_void_p]),
 }
 
 _lib = None

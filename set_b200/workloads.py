@@ -1,0 +1,153 @@
+"""Seeded synthetic problem sets of the benchmark configurations, and the ensemble runner.
+
+The reference measures no dataset; every problem here is a Cartesian box [-1,1]^3 with a LISM
+inflow at x = +1, zero-gradient elsewhere, and a solar-wind source sphere r < 0.125
+(rho = rho_src (0.125/r)^2, radial speed 10, p = 0.01 rho), seeded +-1e-3 perturbations.
+
+  C1  64^3, first-order HLLD, forward Euler, CFL 0.4, 100 steps
+  C2  256^3, minmod + Heun RK2 + HLLD, plain FP64, 200 steps
+  C3  384^3, as C2 in the mixed form, LISM Mach 2-8 and plasma beta 0.1-10 from a seed, 500 steps
+  C4  64 grids, edges log-uniform in [48,160] per axis; inflow speed U[1.5,3], |B| U[0.5,2],
+      tilt U[0,90] deg, source density scale U[20,80]; mixed, 300 steps each; CFL 0.2
+  C5  Poisson arrivals; cubic edges log-uniform in [32,256]; 30% hydro (B = 0, HLLC), 70% MHD
+      (HLLD); LISM as C4; steady state (relative L1 change of rho between 50-step checks below
+      1e-5) or a cap of 3000 steps; CFL 0.2
+
+C4 and C5 use the reference's own CFL factor 0.2 (cuf_solvers.cuf:429): with the strongest
+sources of these draws the second-order Heun/minmod step at 0.4 (the sum over the three
+directions of |S| dt/h is 0.6) is not positivity-robust and produces negative densities.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Batch, CartDesc, LismIC, Solver, StepOpts, cart_desc, lism_ic, lism_prim, step_opts
+
+
+@dataclass
+class Instance:
+    desc: CartDesc
+    ic: LismIC
+    opts: StepOpts
+    steps: int
+    label: str = ""
+
+    @property
+    def cells(self) -> int:
+        return self.desc.nx * self.desc.ny * self.desc.nz
+
+
+def c1_problem(seed: int = 1) -> Instance:
+    return Instance(cart_desc(64), lism_ic(seed=seed), step_opts(n_state=3, order=1, scheme=1, cfl=0.4), 100, "C1")
+
+
+def c2_problem(n: int = 256, seed: int = 2, precision: int = 0) -> Instance:
+    return Instance(cart_desc(n), lism_ic(seed=seed), step_opts(precision=precision), 200, "C2")
+
+
+def c3_problems(count: int = 4, n: int = 384, steps: int = 500, seed: int = 3):
+    """Mixed-form stress cases: LISM Mach in [2,8], plasma beta in [0.1,10] (log-uniform)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        mach = rng.uniform(2.0, 8.0)
+        beta = math.exp(rng.uniform(math.log(0.1), math.log(10.0)))
+        c = math.sqrt(5.0 / 3.0)
+        bmag = math.sqrt(2.0 / beta) * math.sqrt(4 * math.pi)   # beta = 2p/|b|^2, b = B/sqrt(4 pi)
+        inflow = lism_prim(u=(-mach * c, 0.0, 0.0), bmag=bmag)
+        out.append(Instance(cart_desc(n, inflow=inflow), lism_ic(lism=inflow, seed=seed * 1000 + k),
+                            step_opts(precision=1), steps, f"C3 M={mach:.2f} beta={beta:.3g}"))
+    return out
+
+
+def lism_draw(rng, hydro: bool = False):
+    speed = rng.uniform(1.5, 3.0)
+    bmag = 0.0 if hydro else rng.uniform(0.5, 2.0)
+    tilt = rng.uniform(0.0, 90.0)
+    rho_src = rng.uniform(20.0, 80.0)
+    return lism_prim(u=(-speed, 0.0, 0.0), bmag=bmag, tilt_deg=tilt), rho_src
+
+
+def c4_instances(count: int = 64, seed: int = 4, lo: int = 48, hi: int = 160, steps: int = 300,
+                 precision: int = 1, cfl: float = 0.2):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = [int(round(math.exp(rng.uniform(math.log(lo), math.log(hi))))) for _ in range(3)]
+        inflow, rho_src = lism_draw(rng)
+        out.append(Instance(cart_desc(tuple(n), inflow=inflow, rho_src=rho_src),
+                            lism_ic(lism=inflow, seed=seed * 1000 + k), step_opts(precision=precision, cfl=cfl),
+                            steps, f"C4 #{k} {n[0]}x{n[1]}x{n[2]}"))
+    return out
+
+
+@dataclass
+class Request:
+    arrival: float          # seconds after the stream starts
+    inst: Instance
+    steady_tol: float = 1e-5
+    check_every: int = 50
+    max_steps: int = 3000
+
+
+def c5_requests(count: int = 2000, rate: float = 20.0, seed: int = 5, lo: int = 32, hi: int = 256,
+                hydro_frac: float = 0.3, max_steps: int = 3000, cfl: float = 0.2, precision: int = 1):
+    """Poisson request stream, CFL 0.2 (see above; long runs at 256^3 are also not stable at 0.4
+    once the cold wind reaches the outer boundaries)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += rng.exponential(1.0 / rate)
+        n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        hydro = rng.uniform() < hydro_frac
+        inflow, rho_src = lism_draw(rng, hydro)
+        o = step_opts(n_state=2 if hydro else 3, cfl=cfl, precision=precision)
+        inst = Instance(cart_desc(n, inflow=inflow, rho_src=rho_src), lism_ic(lism=inflow, seed=seed * 100000 + k),
+                        o, max_steps, f"C5 #{k} {n}^3 {'hydro' if hydro else 'mhd'}")
+        out.append(Request(t, inst, max_steps=max_steps))
+    return out
+
+
+# ---------------------------------------------------------------------------- ensemble (C4)
+def run_batched(instances, tune: bool = True, keep=None, max_slots=None):
+    """All instances in one batch (same step count); returns wall seconds and optional states."""
+    steps = instances[0].steps
+    assert all(i.steps == steps for i in instances)
+    precision = instances[0].opts.precision
+    with Batch(max_slots or len(instances), precision=precision) as b:
+        slots = [b.add(i.desc, i.ic, i.opts) for i in instances]
+        tuned = b.tune(reps=2) if tune else None
+        b.sync()
+        t0 = time.perf_counter()
+        b.step(steps)
+        b.sync()
+        secs = time.perf_counter() - t0
+        states = {k: b.conserved(slots[k]) for k in (keep or [])}
+        diags = [b.status(s, check=False) for s in slots]
+    return {"seconds": secs, "solves_per_s": len(instances) / secs, "tuned": tuned, "states": states,
+            "cell_updates_per_s": sum(i.cells for i in instances) * steps / secs,
+            "n_negdens": int(sum(d.n_negdens for d in diags)), "fp64_redo": int(sum(d.n_fp64_redo for d in diags))}
+
+
+def run_sequential(instances, precision: int = 0, keep=None):
+    """Each instance alone through the single-solve handle, one after another."""
+    states = {}
+    negdens = 0
+    t0 = time.perf_counter()
+    for k, i in enumerate(instances):
+        o = StepOpts()
+        o.n_state, o.n_disc, o.order, o.scheme, o.precision, o.reserved, o.cfl = (
+            i.opts.n_state, i.opts.n_disc, i.opts.order, i.opts.scheme, precision, 0, i.opts.cfl)
+        with Solver(i.desc, ic=i.ic) as s:
+            s.step(i.steps, o, check=False)
+            negdens += s.status().n_negdens
+            if keep and k in keep:
+                states[k] = s.conserved()
+    secs = time.perf_counter() - t0
+    return {"seconds": secs, "solves_per_s": len(instances) / secs, "states": states, "n_negdens": int(negdens),
+            "cell_updates_per_s": sum(i.cells for i in instances) * instances[0].steps / secs}
