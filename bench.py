@@ -168,6 +168,30 @@ def config_dict(args, reference=False):
             "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single"}
 
 
+def run_mixed_only(args):
+    """`--mixed-only`: only the mixed-form leg (W warm-up and K timed solves); used to profile the
+    mixed kernel in isolation."""
+    import set_b200 as S
+    n, T = args.n, args.tsteps
+    desc = S.cart_desc(n)
+    ic = S.lism_ic(seed=2)
+    o = S.step_opts(n_state=3, order=2, scheme=2, cfl=0.4, precision=1)
+    with S.Solver(desc, ic=ic) as s, S.Solver(desc, ic=ic) as ic_state:
+        for _ in range(args.warmup):
+            s.copy_from(ic_state)
+            s.step(T, o)
+        ms = [0.0, 0.0]
+        cnt = [0, 0]
+        for _ in range(args.steps):
+            s.copy_from(ic_state)
+            _, m, c = s.step_profiled(T, o)
+            ms = [ms[i] + m[i] for i in range(2)]
+            cnt = [cnt[i] + c[i] for i in range(2)]
+    print(json.dumps({"leg": "mixed", "grid": n, "stage1_ms": ms[0] / max(cnt[0], 1),
+                      "stage2_ms": ms[1] / max(cnt[1], 1),
+                      "cell_updates_per_s": n ** 3 * T * args.steps / (sum(ms) / 1e3)}), flush=True)
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -373,6 +397,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--mixed-only", action="store_true")
+    ap.add_argument("--c3", type=int, default=0, help="run config C3 (mixed vs plain) on this many seeded draws")
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--serve-max-edge", type=int, default=96)
     ap.add_argument("--serve-max-steps", type=int, default=600)
@@ -380,6 +406,13 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
+    elif args.mixed_only:
+        run_mixed_only(args)
+    elif args.c3 > 0:
+        import set_b200  # noqa: F401  (fails loudly without the CUDA library)
+        from set_b200 import workloads as WL
+        for r in WL.run_c3(WL.c3_problems(count=args.c3, n=args.n, steps=args.tsteps)):
+            print(json.dumps({"leg": "C3", **r}), flush=True)
     else:
         run_ours(args, world, rank, local)
 

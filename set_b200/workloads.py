@@ -151,3 +151,39 @@ def run_sequential(instances, precision: int = 0, keep=None):
     secs = time.perf_counter() - t0
     return {"seconds": secs, "solves_per_s": len(instances) / secs, "states": states, "n_negdens": int(negdens),
             "cell_updates_per_s": sum(i.cells for i in instances) * instances[0].steps / secs}
+
+
+# ---------------------------------------------------------------------------- mixed vs plain (C3)
+def _prim_fields(U):
+    rho = U[0]
+    ke = 0.5 * (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / rho
+    me = 0.5 * (U[5] ** 2 + U[6] ** 2 + U[7] ** 2) / (4.0 * math.pi)
+    return rho, (U[4] - ke - me) * (5.0 / 3.0 - 1.0), np.sqrt(U[5] ** 2 + U[6] ** 2 + U[7] ** 2)
+
+
+def run_c3(problems):
+    """Each problem run plain (FP64) and mixed from the same initial state; kernel times from
+    CUDA events, L1 errors of rho, p, |B| and the total-energy drift of mixed against plain."""
+    out = []
+    for inst in problems:
+        res = {}
+        for prec in (0, 1):
+            o = StepOpts()
+            o.n_state, o.n_disc, o.order, o.scheme, o.precision, o.reserved, o.cfl = (
+                inst.opts.n_state, 0, 2, 2, prec, 0, inst.opts.cfl)
+            with Solver(inst.desc, ic=inst.ic) as s:
+                t, ms, cnt = s.step_profiled(inst.steps, o)
+                d = s.status()
+                res[prec] = {"U": s.conserved(), "ms": sum(ms), "negdens": d.n_negdens, "redo": d.n_fp64_redo}
+        a = _prim_fields(res[0]["U"])
+        b = _prim_fields(res[1]["U"])
+        l1 = [float(np.abs(y - x).sum() / np.abs(x).sum()) for x, y in zip(a, b)]
+        e64, e32 = res[0]["U"][4].sum(), res[1]["U"][4].sum()
+        out.append({"label": inst.label, "grid": inst.desc.nx, "steps": inst.steps,
+                    "plain_cell_updates_per_s": inst.cells * inst.steps / (res[0]["ms"] / 1e3),
+                    "mixed_cell_updates_per_s": inst.cells * inst.steps / (res[1]["ms"] / 1e3),
+                    "speedup": res[0]["ms"] / res[1]["ms"], "l1_rho": l1[0], "l1_p": l1[1], "l1_bmag": l1[2],
+                    "energy_drift": float(abs(e32 - e64) / abs(e64)),
+                    "n_negdens": [int(res[0]["negdens"]), int(res[1]["negdens"])], "fp64_redo": int(res[1]["redo"])})
+        del res
+    return out
