@@ -175,7 +175,7 @@ def run_mixed_only(args):
     n, T = args.n, args.tsteps
     desc = S.cart_desc(n)
     ic = S.lism_ic(seed=2)
-    o = S.step_opts(n_state=3, order=2, scheme=2, cfl=0.4, precision=1)
+    o = S.step_opts(n_state=3, order=2, scheme=2, cfl=0.4, precision=args.mixed_precision)
     with S.Solver(desc, ic=ic) as s, S.Solver(desc, ic=ic) as ic_state:
         for _ in range(args.warmup):
             s.copy_from(ic_state)
@@ -187,7 +187,7 @@ def run_mixed_only(args):
             _, m, c = s.step_profiled(T, o)
             ms = [ms[i] + m[i] for i in range(2)]
             cnt = [cnt[i] + c[i] for i in range(2)]
-    print(json.dumps({"leg": "mixed", "grid": n, "stage1_ms": ms[0] / max(cnt[0], 1),
+    print(json.dumps({"leg": f"mixed{args.mixed_precision}", "grid": n, "stage1_ms": ms[0] / max(cnt[0], 1),
                       "stage2_ms": ms[1] / max(cnt[1], 1),
                       "cell_updates_per_s": n ** 3 * T * args.steps / (sum(ms) / 1e3)}), flush=True)
 
@@ -398,6 +398,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--mixed-only", action="store_true")
+    ap.add_argument("--mixed-precision", type=int, default=1, choices=[1, 2],
+                    help="mixed form: 1 FP32 Riemann arithmetic, 2 the delta form")
     ap.add_argument("--c3", type=int, default=0, help="run config C3 (mixed vs plain) on this many seeded draws")
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--serve-max-edge", type=int, default=96)

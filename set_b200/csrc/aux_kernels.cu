@@ -64,13 +64,13 @@ __global__ void cons_to_prim_kernel(const GridGeom g, const double* __restrict__
     }
 }
 
-template <typename T, int NSTATE>
+template <typename T, int NSTATE, bool DELTA = false>
 __global__ void chlld_batch_kernel(int64_t n, int n_disc, const double* __restrict__ normals,
                                    const double* __restrict__ w, const double* __restrict__ q1,
                                    const double* __restrict__ q2, double* __restrict__ qqq,
                                    double* __restrict__ speeds, int32_t* __restrict__ flags) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-        chlld_general<T, NSTATE>(normals + 3 * k, w ? w[k] : 0.0, q1 + 8 * k, q2 + 8 * k, n_disc, qqq + 8 * k,
+        chlld_general<T, NSTATE, DELTA>(normals + 3 * k, w ? w[k] : 0.0, q1 + 8 * k, q2 + 8 * k, n_disc, qqq + 8 * k,
                              speeds + 3 * k, flags + k);
     }
 }
@@ -108,7 +108,10 @@ cudaError_t launch_chlld_batch(int64_t n, int n_state, int n_disc, int precision
                                double* speeds, int32_t* flags, cudaStream_t s) {
     const int g = grid_for(n, 128);
 #define SB_LAUNCH(T, NS) chlld_batch_kernel<T, NS><<<g, 128, 0, s>>>(n, n_disc, normals, w, q1, q2, qqq, speeds, flags)
-    if (precision == 1) {
+    if (precision == 2) {
+        if (n_state == 2) chlld_batch_kernel<double, 2, true><<<g, 128, 0, s>>>(n, n_disc, normals, w, q1, q2, qqq, speeds, flags);
+        else chlld_batch_kernel<double, 3, true><<<g, 128, 0, s>>>(n, n_disc, normals, w, q1, q2, qqq, speeds, flags);
+    } else if (precision == 1) {
         switch (n_state) {
             case 0: SB_LAUNCH(float, 0); break;
             case 1: SB_LAUNCH(float, 1); break;

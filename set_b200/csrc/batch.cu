@@ -301,7 +301,7 @@ void free_slot(setb_batch* b, Slot& s) {
 extern "C" {
 
 int32_t setb_batch_create(setb_batch** out, int32_t max_slots, int32_t precision, int64_t hbm_budget) {
-    if (!out || max_slots < 1 || max_slots > 65536 || (precision != 0 && precision != 1) || hbm_budget <= 0)
+    if (!out || max_slots < 1 || max_slots > 65536 || precision < 0 || precision > 2 || hbm_budget <= 0)
         return SETB_EINVAL;
     *out = nullptr;
     int ndev = 0;
@@ -344,7 +344,7 @@ int32_t setb_batch_add(setb_batch* b, const setb_cart_desc* d, const setb_lism_i
     *slot = -1;
     if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->flags != 0 || !(d->dt_init > 0.0)) return SETB_EINVAL;
     if ((o->n_state != 2 && o->n_state != 3) || o->order != 2 || o->scheme != 2 || o->precision != b->precision ||
-        o->reserved != 0 || !(o->cfl > 0.0) || o->n_disc < 0 || o->n_disc > 2)
+        o->reserved != 0 || !(o->cfl > 0.0) || o->n_disc < 0 || o->n_disc > 2 || (o->precision == 2 && o->n_disc != 0))
         return SETB_EINVAL;
     cudaSetDevice(b->device);
     int s = -1;

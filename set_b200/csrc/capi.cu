@@ -61,7 +61,8 @@ int validate_opts(const setb_step_opts* o) {
     if (o->n_disc < 0 || o->n_disc > 2) return SETB_EINVAL;
     if (o->order != 1 && o->order != 2) return SETB_EINVAL;
     if (o->scheme != 1 && o->scheme != 2) return SETB_EINVAL;
-    if (o->precision != 0 && o->precision != 1) return SETB_EINVAL;
+    if (o->precision < 0 || o->precision > 2) return SETB_EINVAL;
+    if (o->precision == 2 && (o->n_state < 2 || o->n_disc != 0)) return SETB_EINVAL;
     if (o->reserved != 0) return SETB_EINVAL;
     if (!(o->cfl > 0.0)) return SETB_EINVAL;
     return SETB_OK;
@@ -279,8 +280,9 @@ int32_t setb_chlld(const int32_t* n_state, const double* al, const double* be, c
 int32_t setb_chlld_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t precision, const double* normals,
                          const double* w, const double* q1, const double* q2, double* qqq, double* speeds,
                          int32_t* flags) {
-    if (n < 0 || n_state < 0 || n_state > 3 || n_disc < 0 || n_disc > 2 || (precision != 0 && precision != 1))
+    if (n < 0 || n_state < 0 || n_state > 3 || n_disc < 0 || n_disc > 2 || precision < 0 || precision > 2)
         return SETB_EINVAL;
+    if (precision == 2 && (n_state < 2 || n_disc != 0)) return SETB_EINVAL;
     if (n == 0) return SETB_OK;
     if (!normals || !q1 || !q2 || !qqq || !speeds || !flags) return SETB_EINVAL;
     int ndev = 0;
@@ -378,9 +380,9 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     StageArgs a{};
     a.g = h->g;
     const int P = o->precision;
-    a.g.lz = choose_lz(h->g, h->sm_count, P ? 2 : 1);
+    a.g.lz = choose_lz(h->g, h->sm_count, P == 1 ? 2 : 1);
     float* comp = nullptr;
-    if (P == 1) {
+    if (P != 0) {
         if (!h->comp) {
             if (cudaMalloc(&h->comp, sizeof(float) * 8 * (size_t)h->g.vs) != cudaSuccess) {
                 cudaGetLastError();

@@ -191,7 +191,7 @@ SB_HD void lism_cell(const GridGeom& g, const double* lism, uint64_t seed, doubl
 // General-normal chlld for a batch of faces: the lab states are rotated into an orthonormal
 // face frame (the reference's basis construction, Solvers.f90:1236-1273), solved, and the
 // momentum / B fluxes rotated back.
-template <typename T, int NSTATE>
+template <typename T, int NSTATE, bool DELTA = false>
 SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const double* q2d, int n_disc,
                           double* qqq, double* sp, int32_t* flag) {
     const double al = nrm[0], be = nrm[1], ge = nrm[2];
@@ -237,10 +237,24 @@ SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const d
         o[6] = T(q[5] * e2[0] + q[6] * e2[1] + q[7] * e2[2]);
         o[7] = T(q[5] * e3[0] + q[6] * e3[1] + q[7] * e3[2]);
     }
-    int fl = riemann<T, NSTATE, true, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
+    int fl;
+    if (DELTA && sizeof(T) == 8 && w == 0.0 && NSTATE >= 2 && n_disc == 0) {
+        float SLf, SRf, SMf;
+        double Fd[8];
+        fl = riemann_delta<(NSTATE >= 2 ? NSTATE : 3)>((const double*)a, (const double*)b, Fd, SLf, SRf, SMf);
+        for (int k = 0; k < 8; k++) F[k] = (T)Fd[k];
+        SL = (T)SLf;
+        SR = (T)SRf;
+        SM = (T)SMf;
+        if (fl & kFlagStar) {
+            fl = riemann<T, NSTATE, true, false>(a, b, T(w), n_disc, F, SL, SR, SM) | kFlagStar;
+        }
+    } else {
+        fl = riemann<T, NSTATE, true, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
+    }
     if (sizeof(T) == 4 && (fl & kFlagStar)) {
         // the mixed form's rule: a face whose FP32 star state is not positive is redone in FP64
-        chlld_general<double, NSTATE>(nrm, w, q1d, q2d, n_disc, qqq, sp, flag);
+        chlld_general<double, NSTATE, false>(nrm, w, q1d, q2d, n_disc, qqq, sp, flag);
         *flag |= kFlagStar;
         return;
     }

@@ -38,7 +38,6 @@ constexpr int NXF = (TX + 1) * TY;        // x faces
 constexpr int NYF = TX * (TY + 1);        // y faces
 constexpr int NF = NZF + NXF + NYF;
 constexpr int RING = 4;
-constexpr int SMEM_ELEMS = RING * 8 * PLANE + 8 * (NZF + NXF + NYF);
 
 __device__ __forceinline__ int ring_slot(int k) { return (k + 4 * RING) & (RING - 1); }
 
@@ -102,14 +101,50 @@ __device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j
 // the solve's clock.  Called by the single-solve kernel (one tile per CTA) and by the batch
 // kernel (tiles of many solves drawn from a work queue); every CTA-wide barrier is reached by all
 // threads, and the function ends with one so a CTA may run the next tile immediately.
+// Storage and arithmetic types of the two forms: ring (primitives), flux buffer, Riemann math.
+template <int P> struct Types {
+    using Ring = double;
+    using Flux = double;
+    using Math = double;
+};
+template <> struct Types<2> {   // delta form: FP64 states and fluxes, FP32 inside the solver
+    using Ring = double;
+    using Flux = double;
+    using Math = double;
+};
+template <> struct Types<1> {
+#if defined(SB_MIXED_RING_FP64)
+    using Ring = double;
+#else
+    using Ring = float;
+#endif
+#if defined(SB_MIXED_FLUX_FP64)
+    using Flux = double;
+#else
+    using Flux = float;
+#endif
+    using Math = float;
+};
+
+// FP64 recompute of a face of the delta form from its (FP64) face states; out of line so the
+// main path keeps its registers.
+template <int NSTATE>
+__device__ __noinline__ int face_fp64_states(const double* q1, const double* q2, int n_disc, double* F, double* sl,
+                                             double* sr) {
+    double SM;
+    return riemann<double, NSTATE, false, false>(q1, q2, 0.0, n_disc, F, *sl, *sr, SM);
+}
+
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
 __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int bz, unsigned total_tiles) {
-    using RT = typename std::conditional<P == 0, double, float>::type;
+    using RG = typename Types<P>::Ring;
+    using FT = typename Types<P>::Flux;
+    using RT = typename Types<P>::Math;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    RT* ring = reinterpret_cast<RT*>(smem_raw);
-    RT* fz = ring + RING * 8 * PLANE;   // [8][NZF]
-    RT* fx = fz + 8 * NZF;              // [8][NXF]
-    RT* fy = fx + 8 * NXF;              // [8][NYF]
+    RG* ring = reinterpret_cast<RG*>(smem_raw);
+    FT* fz = reinterpret_cast<FT*>(ring + RING * 8 * PLANE);   // [8][NZF]
+    FT* fx = fz + 8 * NZF;                                      // [8][NXF]
+    FT* fy = fx + 8 * NXF;                                      // [8][NYF]
     __shared__ double red[NT / 32];
     __shared__ unsigned long long cnt[5];
     __shared__ bool last_cta;
@@ -131,8 +166,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     // the dt candidate (min is idempotent) but not the diagnostic counters.
     auto do_face = [&](int f, int k, bool dup) {
         int axis, cLL, cL, cR, cRR, fxx, fyy, gk;
-        const RT *sLL, *sL, *sR, *sRR;
-        RT* out;
+        const RG *sLL, *sL, *sR, *sRR;
+        FT* out;
         int oidx, ostride;
         bool real;
         if (f < NZF) {
@@ -186,35 +221,50 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 #pragma unroll
         for (int v = 0; v < 8; v++) {
             const int o = perm[v] * PLANE;
-            qL[v] = sL[o + cL];
-            qR[v] = sR[o + cR];
+            qL[v] = (RT)sL[o + cL];
+            qR[v] = (RT)sR[o + cR];
             if (v < 5) {
-                qLL[v] = sLL[o + cLL];
-                qRR[v] = sRR[o + cRR];
+                qLL[v] = (RT)sLL[o + cLL];
+                qRR[v] = (RT)sRR[o + cRR];
             } else {
                 qLL[v] = RT(0);
                 qRR[v] = RT(0);
             }
         }
-        RT q1[8], q2[8], F[8], SL, SR, SM;
+        RT q1[8], q2[8], F[8];
         reconstruct<RT, ORDER>(qLL, qL, qR, qRR, q1, q2);
         if (real && !dup && (q1[0] < RT(0) || q2[0] < RT(0))) n_recon++;
-        int fl = riemann<RT, NSTATE, false, P == 1>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
-        double sl = (double)SL, sr = (double)SR;
+        int fl;
+        double sl, sr;
+        if constexpr (P == 2) {
+            float SLf, SRf, SMf;
+            fl = riemann_delta<NSTATE>(q1, q2, F, SLf, SRf, SMf);
+            sl = (double)SLf;
+            sr = (double)SRf;
+            if (fl & kFlagStar) {
+                fl = face_fp64_states<NSTATE>(q1, q2, A.n_disc, F, &sl, &sr);
+                if (real && !dup) n_redo++;
+            }
+        } else {
+            RT SL, SR, SM;
+            fl = riemann<RT, NSTATE, false, P == 1>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+            sl = (double)SL;
+            sr = (double)SR;
+        }
         const double sq = g.square[axis];
         if (P == 1 && real && (fl & kFlagStar)) {
             double F64[8];
             fl = face_fp64<NSTATE, ORDER>(A, axis, i0 + fxx, j0 + fyy, gk, F64, &sl, &sr);
             if (!dup) n_redo++;
 #pragma unroll
-            for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (RT)(F64[v] * sq);
+            for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (FT)(F64[v] * sq);
         } else {
             if (fl & kFlagWave) {
 #pragma unroll
                 for (int v = 0; v < 8; v++) F[v] = RT(0);
             }
 #pragma unroll
-            for (int v = 0; v < 8; v++) out[perm[v] * ostride + oidx] = (RT)(F[v] * (RT)sq);
+            for (int v = 0; v < 8; v++) out[perm[v] * ostride + oidx] = (FT)(F[v] * (RT)sq);
         }
         if ((fl & kFlagWave) && real && !dup) n_wave++;
         if (WANT_DT && real) rate = fmax(rate, fmax(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
@@ -223,12 +273,12 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     // ---- the march.  Iteration k0-1 is the prologue: planes k0-2 .. k0+1 and only the z face
     // k0-1/2 (carried into the first update).  Every face goes through the one do_face call
     // site below, so a face's arithmetic does not depend on where a chunk starts.
-    for (int kk = k0 - 2; kk <= k0; kk++) load_plane<RT>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
+    for (int kk = k0 - 2; kk <= k0; kk++) load_plane<RG>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
     double fzl[8];
     const int gi = i0 + tx, gj = j0 + ty;
     const bool own = (gi < g.nx) && (gj < g.ny);
     for (int k = k0 - 1; k < k1; k++) {
-        load_plane<RT>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
+        load_plane<RG>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
         __syncthreads();
         const bool pro = (k < k0);
         const int nf = pro ? NZF : NF;
@@ -262,7 +312,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                     pot = pot + fzh[v];
                     uin[v] = A.Uin[v * g.vs + off];
                     const double inc = dt * (pot * g.inv_vol);
-                    if (P == 1 && A.comp) {
+                    if (P != 0 && A.comp) {
                         // compensated sum U_new = base + delta (cuf_solvers.cuf:741-770 as an
                         // increment); the FP32 compensation carries the rounding of the add
                         const double base = KIND == 0 ? uin[v] : A.Ubase[v * g.vs + off];
@@ -292,12 +342,12 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                         cmp[4] = 0.0;
                     }
                 }
-                if (P == 1 && A.comp && !reset_comp) {
+                if (P != 0 && A.comp && !reset_comp) {
 #pragma unroll
                     for (int v = 0; v < 8; v++) A.comp[v * g.vs + off] = (float)cmp[v];
                 }
             }
-            if (P == 1 && A.comp && reset_comp) {
+            if (P != 0 && A.comp && reset_comp) {
 #pragma unroll
                 for (int v = 0; v < 8; v++) A.comp[v * g.vs + off] = 0.0f;
             }
@@ -353,7 +403,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageArgs A) {
+__global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) stage_kernel(const StageArgs A) {
     run_tile<P, NSTATE, ORDER, KIND, WANT_DT>(A, blockIdx.x, blockIdx.y, blockIdx.z,
                                                gridDim.x * gridDim.y * gridDim.z);
 }
@@ -362,7 +412,7 @@ __global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) stage_kernel(const StageAr
 // tile's solve selects the arguments (copied to shared memory) and the Riemann solver.  The
 // items of one solve are counted by its own clock, so every solve keeps its own lagged dt.
 template <int P, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) batch_stage_kernel(const BatchArgs B) {
+__global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) batch_stage_kernel(const BatchArgs B) {
     __shared__ __align__(16) StageArgs As;
     __shared__ int4 it;
     constexpr int WORDS = sizeof(StageArgs) / sizeof(unsigned long long);
@@ -388,7 +438,8 @@ __global__ void __launch_bounds__(NT, P == 0 ? 1 : 2) batch_stage_kernel(const B
 
 template <int P>
 constexpr int smem_bytes() {
-    return SMEM_ELEMS * (P == 0 ? (int)sizeof(double) : (int)sizeof(float));
+    return RING * 8 * PLANE * (int)sizeof(typename Types<P>::Ring) +
+           8 * (NZF + NXF + NYF) * (int)sizeof(typename Types<P>::Flux);
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
@@ -436,35 +487,45 @@ cudaError_t batch_attr() {
 
 cudaError_t prepare_batch_kernels(int precision) {
     cudaError_t e;
-    if (precision) {
+    if (precision == 1) {
         if ((e = batch_attr<1, 0, true>()) != cudaSuccess) return e;
         return batch_attr<1, 1, false>();
+    }
+    if (precision == 2) {
+        if ((e = batch_attr<2, 0, true>()) != cudaSuccess) return e;
+        return batch_attr<2, 1, false>();
     }
     if ((e = batch_attr<0, 0, true>()) != cudaSuccess) return e;
     return batch_attr<0, 1, false>();
 }
 
-int batch_ctas_per_sm(int precision) { return precision ? 2 : 1; }
+int batch_ctas_per_sm(int precision) { return precision == 1 ? 2 : 1; }
+
+template <int P>
+void launch_batch_p(const BatchArgs& b, int kind, bool want_dt, int grid, cudaStream_t s) {
+    if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P>(), s>>>(b);
+    else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P>(), s>>>(b);
+}
 
 cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
                                cudaStream_t s) {
-    if (precision) {
-        if (kind == 0 && want_dt) batch_stage_kernel<1, 2, 0, true><<<grid, NT, smem_bytes<1>(), s>>>(b);
-        else batch_stage_kernel<1, 2, 1, false><<<grid, NT, smem_bytes<1>(), s>>>(b);
-    } else {
-        if (kind == 0 && want_dt) batch_stage_kernel<0, 2, 0, true><<<grid, NT, smem_bytes<0>(), s>>>(b);
-        else batch_stage_kernel<0, 2, 1, false><<<grid, NT, smem_bytes<0>(), s>>>(b);
-    }
+    if (precision == 1) launch_batch_p<1>(b, kind, want_dt, grid, s);
+    else if (precision == 2) launch_batch_p<2>(b, kind, want_dt, grid, s);
+    else launch_batch_p<0>(b, kind, want_dt, grid, s);
     return cudaGetLastError();
 }
 
-int stage_smem_bytes(int precision) { return precision ? smem_bytes<1>() : smem_bytes<0>(); }
+int stage_smem_bytes(int precision) {
+    return precision == 1 ? smem_bytes<1>() : (precision == 2 ? smem_bytes<2>() : smem_bytes<0>());
+}
 int stage_fp64_smem_bytes() { return smem_bytes<0>(); }
 
 cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
                          cudaStream_t s) {
-    return precision ? launch_p<1>(a, n_state, order, kind, want_dt, s)
-                     : launch_p<0>(a, n_state, order, kind, want_dt, s);
+    if (precision == 1) return launch_p<1>(a, n_state, order, kind, want_dt, s);
+    if (precision == 2)   // the delta form covers HLLC (n_state 2) and HLLD (n_state 3)
+        return n_state == 2 ? launch_n<2, 2>(a, order, kind, want_dt, s) : launch_n<2, 3>(a, order, kind, want_dt, s);
+    return launch_p<0>(a, n_state, order, kind, want_dt, s);
 }
 
 cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int kind, bool want_dt,

@@ -161,13 +161,14 @@ def _prim_fields(U):
     return rho, (U[4] - ke - me) * (5.0 / 3.0 - 1.0), np.sqrt(U[5] ** 2 + U[6] ** 2 + U[7] ** 2)
 
 
-def run_c3(problems):
-    """Each problem run plain (FP64) and mixed from the same initial state; kernel times from
-    CUDA events, L1 errors of rho, p, |B| and the total-energy drift of mixed against plain."""
+def run_c3(problems, mixed=(1, 2)):
+    """Each problem run plain (FP64) and in each mixed form (1: FP32 Riemann arithmetic; 2: the
+    delta form) from the same initial state; kernel times from CUDA events, L1 errors of rho, p,
+    |B| and the total-energy drift against plain."""
     out = []
     for inst in problems:
         res = {}
-        for prec in (0, 1):
+        for prec in (0,) + tuple(mixed):
             o = StepOpts()
             o.n_state, o.n_disc, o.order, o.scheme, o.precision, o.reserved, o.cfl = (
                 inst.opts.n_state, 0, 2, 2, prec, 0, inst.opts.cfl)
@@ -176,14 +177,18 @@ def run_c3(problems):
                 d = s.status()
                 res[prec] = {"U": s.conserved(), "ms": sum(ms), "negdens": d.n_negdens, "redo": d.n_fp64_redo}
         a = _prim_fields(res[0]["U"])
-        b = _prim_fields(res[1]["U"])
-        l1 = [float(np.abs(y - x).sum() / np.abs(x).sum()) for x, y in zip(a, b)]
-        e64, e32 = res[0]["U"][4].sum(), res[1]["U"][4].sum()
-        out.append({"label": inst.label, "grid": inst.desc.nx, "steps": inst.steps,
-                    "plain_cell_updates_per_s": inst.cells * inst.steps / (res[0]["ms"] / 1e3),
-                    "mixed_cell_updates_per_s": inst.cells * inst.steps / (res[1]["ms"] / 1e3),
-                    "speedup": res[0]["ms"] / res[1]["ms"], "l1_rho": l1[0], "l1_p": l1[1], "l1_bmag": l1[2],
-                    "energy_drift": float(abs(e32 - e64) / abs(e64)),
-                    "n_negdens": [int(res[0]["negdens"]), int(res[1]["negdens"])], "fp64_redo": int(res[1]["redo"])})
+        e64 = res[0]["U"][4].sum()
+        row = {"label": inst.label, "grid": inst.desc.nx, "steps": inst.steps,
+               "plain_cell_updates_per_s": inst.cells * inst.steps / (res[0]["ms"] / 1e3),
+               "plain_n_negdens": int(res[0]["negdens"])}
+        for prec in mixed:
+            b = _prim_fields(res[prec]["U"])
+            l1 = [float(np.abs(y - x).sum() / np.abs(x).sum()) for x, y in zip(a, b)]
+            row[f"mixed{prec}"] = {
+                "cell_updates_per_s": inst.cells * inst.steps / (res[prec]["ms"] / 1e3),
+                "speedup": res[0]["ms"] / res[prec]["ms"], "l1_rho": l1[0], "l1_p": l1[1], "l1_bmag": l1[2],
+                "energy_drift": float(abs(res[prec]["U"][4].sum() - e64) / abs(e64)),
+                "n_negdens": int(res[prec]["negdens"]), "fp64_redo": int(res[prec]["redo"])}
+        out.append(row)
         del res
     return out

@@ -99,3 +99,61 @@ def test_mixed_is_deterministic():
             s.step(10, S.step_opts(precision=1))
             out.append(s.conserved())
     np.testing.assert_array_equal(out[0], out[1])
+
+
+# ------------------------------------------------------------------ delta form (precision 2)
+def test_delta_form_solver_is_accurate_on_nearby_states():
+    # smooth-flow faces: q2 = q1 (1 + 1e-3 noise).  FP32 arithmetic on full states leaves
+    # ~1e-7 |F| per flux; the delta form keeps FP32 on the differences only.
+    rng = np.random.default_rng(51)
+    n = 4000
+    q1 = np.array([[rng.uniform(0.2, 3), *rng.normal(0, 1.5, 3), rng.uniform(0.2, 3), *rng.normal(0, 2, 3)]
+                   for _ in range(n)])
+    q2 = q1 * (1.0 + 1e-3 * rng.normal(size=q1.shape))
+    nr = np.eye(3)[rng.integers(0, 3, n)]
+    ref = np.array([O.chlld(3, nr[k], 0.0, q1[k], q2[k])[1] for k in range(n)])
+    scale = np.abs(ref).max(axis=1)
+    f32, _, _ = S.chlld_batch(3, nr, q1, q2, precision=1)
+    fd, _, fl = S.chlld_batch(3, nr, q1, q2, precision=2)
+    e32 = np.abs(f32 - ref).max(axis=1) / scale
+    ed = np.abs(fd - ref).max(axis=1) / scale
+    print(f"nearby states: fp32 median {np.median(e32):.2e} max {e32.max():.2e}; "
+          f"delta median {np.median(ed):.2e} max {ed.max():.2e}")
+    assert (fl & 1).sum() == 0
+    assert np.median(ed) < 1e-10 and ed.max() < 1e-8
+    assert np.median(ed) < 1e-3 * np.median(e32)
+
+
+def test_delta_form_matches_fp64_on_random_states():
+    rng = np.random.default_rng(52)
+    n = 3000
+    q1 = np.array([[rng.uniform(0.1, 4), *rng.normal(0, 1.5, 3), rng.uniform(0.05, 4), *rng.normal(0, 2, 3)]
+                   for _ in range(n)])
+    q2 = np.array([[rng.uniform(0.1, 4), *rng.normal(0, 1.5, 3), rng.uniform(0.05, 4), *rng.normal(0, 2, 3)]
+                   for _ in range(n)])
+    nr = np.eye(3)[rng.integers(0, 3, n)]
+    ref = np.array([O.chlld(3, nr[k], 0.0, q1[k], q2[k])[1] for k in range(n)])
+    fd, _, fl = S.chlld_batch(3, nr, q1, q2, precision=2)
+    ed = np.abs(fd - ref).max(axis=1) / np.abs(ref).max(axis=1)
+    assert (fl & 1).sum() == 0
+    assert np.all(ed[(fl & 2) != 0] <= 1e-12)          # recomputed in FP64
+    assert np.median(ed) < 1e-6 and ed.max() < 1e-3
+
+
+@pytest.mark.parametrize("mach,beta", [(2.0, 10.0), (8.0, 0.1)])
+def test_delta_form_100_steps_l1_vs_fp64(mach, beta):
+    c = np.sqrt(5.0 / 3.0)
+    bmag = np.sqrt(2.0 / beta) * np.sqrt(4 * np.pi)
+    inflow = S.lism_prim(u=(-mach * c, 0.0, 0.0), bmag=bmag)
+    desc = S.cart_desc(48, inflow=inflow)
+    ic = S.lism_ic(lism=inflow, seed=31)
+    res = {}
+    for prec in (0, 2):
+        with S.Solver(desc, ic=ic) as s:
+            s.step(100, S.step_opts(precision=prec))
+            res[prec] = s.conserved()
+    r64, p64, b64 = prim_fields(res[0])
+    rd, pd, bd = prim_fields(res[2])
+    e_rho, e_p, e_b = rel_l1(rd, r64), rel_l1(pd, p64), rel_l1(bd, b64)
+    print(f"delta form mach {mach} beta {beta}: L1 rho {e_rho:.2e} p {e_p:.2e} |B| {e_b:.2e}")
+    assert e_rho <= 1e-7 and e_p <= 1e-6 and e_b <= 1e-6
