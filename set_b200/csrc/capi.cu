@@ -62,7 +62,7 @@ int validate_opts(const setb_step_opts* o) {
     if (o->order != 1 && o->order != 2) return SETB_EINVAL;
     if (o->scheme != 1 && o->scheme != 2) return SETB_EINVAL;
     if (o->precision < 0 || o->precision > 2) return SETB_EINVAL;
-    if (o->precision == 2 && (o->n_state < 2 || o->n_disc != 0)) return SETB_EINVAL;
+    if (o->precision >= 2 && (o->n_state < 2 || o->n_disc != 0)) return SETB_EINVAL;
     if (o->reserved != 0) return SETB_EINVAL;
     if (!(o->cfl > 0.0)) return SETB_EINVAL;
     return SETB_OK;
@@ -282,7 +282,7 @@ int32_t setb_chlld_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t pre
                          int32_t* flags) {
     if (n < 0 || n_state < 0 || n_state > 3 || n_disc < 0 || n_disc > 2 || precision < 0 || precision > 2)
         return SETB_EINVAL;
-    if (precision == 2 && (n_state < 2 || n_disc != 0)) return SETB_EINVAL;
+    if (precision >= 2 && (n_state < 2 || n_disc != 0)) return SETB_EINVAL;
     if (n == 0) return SETB_OK;
     if (!normals || !q1 || !q2 || !qqq || !speeds || !flags) return SETB_EINVAL;
     int ndev = 0;
@@ -380,7 +380,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     StageArgs a{};
     a.g = h->g;
     const int P = o->precision;
-    a.g.lz = choose_lz(h->g, h->sm_count, P == 1 ? 2 : 1);
+    a.g.lz = choose_lz(h->g, h->sm_count, batch_ctas_per_sm(P));
     float* comp = nullptr;
     if (P != 0) {
         if (!h->comp) {

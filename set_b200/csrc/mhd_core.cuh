@@ -398,43 +398,36 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
 // ------------------------------------------------------------------ delta-form solver
 // The same HLLD (NSTATE 3) / HLLC-without-field (NSTATE 2) flux, arranged so that FP32 only
 // computes small quantities.  In FP32 arithmetic on full-magnitude states every flux carries
-// ~6e-8 |F| of rounding whatever its storage; here the face states and the physical flux of the
-// selected side stay FP64, and FP32 evaluates the wave speeds, the jumps across the face and the
-// differences between each star state and its side state, all in closed form:
+// ~6e-8 |F| of rounding whatever its storage; here FP32 evaluates the wave speeds, the jumps
+// across the face and the differences between each star state and its side state, all in closed
+// form:
 //   SM - u1 = (suR r2 du - dpt) / (suR r2 - suL r1),      SM - u2 = (suL r1 du - dpt) / (...)
 //   rho*L - r1 = r1 (SM - u1) / (SL - SM),                tb - 1 = r suL (SM - u1) / tt
 //   pt* - ptL = (r1 r2 suR suL du - suL r1 dpt) / (...), bn - bx1 = SR dbx / (SR - SL)
 //   e*L - e1 = ((e1 + pt*)(SM - u1) + (pt* - ptL) u1 + bn (v.b - v*.b*)) / (SL - SM)
 // and likewise for the double-star states (Solvers.f90:1600-1718).  The flux is
-// F = F_side (FP64) + S2 (U** - U*) + S1 (U* - U_side) with the bracketed differences in FP32.
-// Returns kFlagWave / kFlagStar like riemann(); kFlagStar also when NSTATE 2 sees a magnetic
-// field (the delta form covers hydro HLLC only) -- the caller then recomputes the face in FP64.
-template <int NSTATE>
-SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SLo, float& SRo, float& SMo) {
-    typedef float f;
-    const double ispi4 = kInvSpi4;
-    const double r1 = q1[0], u1 = q1[1], v1 = q1[2], w1 = q1[3], p1 = q1[4];
-    const double bx1 = q1[5] * ispi4, by1 = q1[6] * ispi4, bz1 = q1[7] * ispi4;
-    const double r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
-    const double bx2 = q2[5] * ispi4, by2 = q2[6] * ispi4, bz2 = q2[7] * ispi4;
-    const double b2L = (bx1 * bx1 + by1 * by1) + bz1 * bz1;
-    const double b2R = (bx2 * bx2 + by2 * by2) + bz2 * bz2;
-    const double ptL = p1 + 0.5 * b2L, ptR = p2 + 0.5 * b2R;
-    if (NSTATE == 2 && (b2L != 0.0 || b2R != 0.0)) return kFlagStar;
+// F = F_side + S2 (U** - U*) + S1 (U* - U_side); delta_core returns the bracketed part (the
+// dissipation of the selected side, FP32) and the caller adds the physical flux of that side.
+struct DeltaIn {   // FP32 side values (b = B / sqrt(4 pi)), their jumps, energies, total pressure
+    float r1, u1, v1, w1, p1, bx1, by1, bz1, b2L, e1, ptL;
+    float r2, u2, v2, w2, p2, bx2, by2, bz2, b2R, e2;
+    float du, dv, dw, dbx, dby, dbz, dpt;
+};
 
-    // FP32 side values (multipliers of small quantities) and FP64-formed jumps
-    const f fr1 = (f)r1, fu1 = (f)u1, fv1 = (f)v1, fw1 = (f)w1;
-    const f fr2 = (f)r2, fu2 = (f)u2, fv2 = (f)v2, fw2 = (f)w2;
-    const f fbx1 = (f)bx1, fby1 = (f)by1, fbz1 = (f)bz1, fbx2 = (f)bx2, fby2 = (f)by2, fbz2 = (f)bz2;
-    const f du = (f)(u2 - u1), dv = (f)(v2 - v1), dw = (f)(w2 - w1);
-    const f dbx = (f)(bx2 - bx1), dby = (f)(by2 - by1), dbz = (f)(bz2 - bz1);
-    const f dpt = (f)(ptR - ptL);
+// Returns kFlagWave / kFlagStar like riemann() and sets `right` (the selected side) and c[8]:
+// the flux minus the physical flux of the selected side, c[5] the whole normal-field flux.
+template <int NSTATE>
+SB_HD int delta_core(const DeltaIn& d, float* c, bool& right, float& SLo, float& SRo, float& SMo) {
+    typedef float f;
+    const f fr1 = d.r1, fu1 = d.u1, fv1 = d.v1, fw1 = d.w1, fr2 = d.r2, fu2 = d.u2, fv2 = d.v2, fw2 = d.w2;
+    const f fbx1 = d.bx1, fby1 = d.by1, fbz1 = d.bz1, fbx2 = d.bx2, fby2 = d.by2, fbz2 = d.bz2;
+    const f du = d.du, dv = d.dv, dw = d.dw, dbx = d.dbx, dby = d.dby, dbz = d.dbz, dpt = d.dpt;
 
     // fast speeds (as riemann())
     const f ga = (f)kGamma, half = 0.5f;
     const f ir1 = sb_rcp(fr1), ir2 = sb_rcp(fr2);
-    const f c2L = ga * (f)p1 * ir1, c2R = ga * (f)p2 * ir2;
-    const f sL = c2L + (f)b2L * ir1, sR = c2R + (f)b2R * ir2;
+    const f c2L = ga * d.p1 * ir1, c2R = ga * d.p2 * ir2;
+    const f sL = c2L + d.b2L * ir1, sR = c2R + d.b2R * ir2;
     const f cfL = sb_sqrt(half * (sL + sb_sqrt(sb_pos(sL * sL - 4.0f * c2L * (fbx1 * fbx1 * ir1)))));
     const f cfR = sb_sqrt(half * (sR + sb_sqrt(sb_pos(sR * sR - 4.0f * c2R * (fbx2 * fbx2 * ir2)))));
 
@@ -453,8 +446,6 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
     const f islm = sb_rcp(slm), isrm = sb_rcp(srm);
     const f D0L = fr1 * dL * islm, D0R = fr2 * dR * isrm;   // rho* - rho
     const f rzL = fr1 + D0L, rzR = fr2 + D0R;
-    const double e1 = (p1 * kInvG1 + r1 * (0.5 * ((u1 * u1 + v1 * v1) + w1 * w1))) + 0.5 * b2L;
-    const double e2 = (p2 * kInvG1 + r2 * (0.5 * ((u2 * u2 + v2 * v2) + w2 * w2))) + 0.5 * b2R;
 
     f DL[8], DR[8], DDL[8], DDR[8];   // U* - U_side, U** - U*
     f SZL = SM, SZR = SM, ptz, bn = 0.0f, bz2L = 0.f, bz3L = 0.f, bz2R = 0.f, bz3R = 0.f;
@@ -464,11 +455,11 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
     if (NSTATE == 2) {   // HLLC without field: v* = v, B* = 0
         const f ptz_m_ptL = half * ((dpt + fr2 * suR * dR) + fr1 * suL * dL);
         const f ptz_m_ptR = ptz_m_ptL - dpt;
-        ptz = (f)ptL + ptz_m_ptL;
+        ptz = d.ptL + ptz_m_ptL;
         DL[0] = D0L; DL[1] = D0L * SM + fr1 * dL; DL[2] = D0L * fv1; DL[3] = D0L * fw1;
-        DL[4] = (((f)e1 + ptz) * dL + ptz_m_ptL * fu1) * islm;
+        DL[4] = ((d.e1 + ptz) * dL + ptz_m_ptL * fu1) * islm;
         DR[0] = D0R; DR[1] = D0R * SM + fr2 * dR; DR[2] = D0R * fv2; DR[3] = D0R * fw2;
-        DR[4] = (((f)e2 + ptz) * dR + ptz_m_ptR * fu2) * isrm;
+        DR[4] = ((d.e2 + ptz) * dR + ptz_m_ptR * fu2) * isrm;
 #pragma unroll
         for (int k = 5; k < 8; k++) DL[k] = DR[k] = 0.0f;
 #pragma unroll
@@ -485,7 +476,7 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
         const f bn2 = bn * bn;
         const f ptz_m_ptL = (fr1 * fr2 * suR * suL * du - suL * fr1 * dpt) * iden;
         const f ptz_m_ptR = ptz_m_ptL - dpt;
-        ptz = (f)ptL + ptz_m_ptL;
+        ptz = d.ptL + ptz_m_ptL;
         // left star
         const f ttL = fr1 * suL * slm - bn2;
         f tvL = 0.0f, tbL = -1.0f;   // tv and tb - 1 (degenerate: tv = tb = 0)
@@ -501,7 +492,7 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
         bz3L = fbz1 + dbL3;
         const f dsL = -(dL * fbx1 + SM * bnL) - (fv1 * dbL2 + dvL2 * bz2L) - (fw1 * dbL3 + dvL3 * bz3L);
         DL[0] = D0L; DL[1] = D0L * SM + fr1 * dL; DL[2] = D0L * vzL2 + fr1 * dvL2; DL[3] = D0L * vzL3 + fr1 * dvL3;
-        DL[4] = (((f)e1 + ptz) * dL + ptz_m_ptL * fu1 + bn * dsL) * islm;
+        DL[4] = ((d.e1 + ptz) * dL + ptz_m_ptL * fu1 + bn * dsL) * islm;
         DL[5] = bnL; DL[6] = dbL2; DL[7] = dbL3;
         // right star
         const f ttR = fr2 * suR * srm - bn2;
@@ -518,7 +509,7 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
         bz3R = fbz2 + dbR3;
         const f dsR = -(dR * fbx2 + SM * bnR) - (fv2 * dbR2 + dvR2 * bz2R) - (fw2 * dbR3 + dvR3 * bz3R);
         DR[0] = D0R; DR[1] = D0R * SM + fr2 * dR; DR[2] = D0R * vzR2 + fr2 * dvR2; DR[3] = D0R * vzR3 + fr2 * dvR3;
-        DR[4] = (((f)e2 + ptz) * dR + ptz_m_ptR * fu2 + bn * dsR) * isrm;
+        DR[4] = ((d.e2 + ptz) * dR + ptz_m_ptR * fu2 + bn * dsR) * isrm;
         DR[5] = bnR; DR[6] = dbR2; DR[7] = dbR3;
         // double star
         const f isR = sb_rsqrt(rzR), isL = sb_rsqrt(rzL);
@@ -554,7 +545,7 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
         else region = 0;
     }
     int flag = region == 0 ? kFlagWave : 0;
-    const bool right = region >= 4;
+    right = region >= 4;
     const bool use1 = (region >= 2 && region <= 5), use2 = (region == 3 || region == 4);
     // positivity of the selected star state (rho* > 0, p* = pt* - |b*|^2 / 2 > 0)
     if (use1) {
@@ -562,33 +553,61 @@ SB_HD int riemann_delta(const double* q1, const double* q2, double* F, float& SL
         const f b2 = use2 ? bzz2 : (right ? bz2R : bz2L), b3 = use2 ? bzz3 : (right ? bz3R : bz3L);
         if (!(rz > 0.0f) || !(ptz - half * ((bn * bn + b2 * b2) + b3 * b3) > 0.0f)) flag |= kFlagStar;
     }
-    // physical flux of the selected side, FP64
-    const double r = right ? r2 : r1, u = right ? u2 : u1, v = right ? v2 : v1, w = right ? w2 : w1;
-    const double bx = right ? bx2 : bx1, by = right ? by2 : by1, bz = right ? bz2 : bz1;
-    const double pt = right ? ptR : ptL, e = right ? e2 : e1;
-    const double m = r * u;
-    double Fs[8];
-    Fs[0] = m;
-    Fs[1] = (m * u + pt) - bx * bx;
-    Fs[2] = m * v - bx * by;
-    Fs[3] = m * w - bx * bz;
-    Fs[4] = (e + pt) * u - bx * ((u * bx + v * by) + w * bz);
-    Fs[5] = 0.0;
-    Fs[6] = u * by - v * bx;
-    Fs[7] = u * bz - w * bx;
     const f S1 = right ? SR : SL, S2 = right ? SZR : SZL;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        f c = 0.0f;
-        if (use2) c = S2 * (right ? DDR[k] : DDL[k]);
-        if (use1) c = c + S1 * (right ? DR[k] : DL[k]);
-        F[k] = Fs[k] + (double)c;
+        f ck = 0.0f;
+        if (use2) ck = S2 * (right ? DDR[k] : DDL[k]);
+        if (use1) ck = ck + S1 * (right ? DR[k] : DL[k]);
+        c[k] = ck;
     }
-    if (NSTATE == 3) F[5] = (double)(-sb_max(sb_abs(SL), sb_abs(SR)) * dbx);
-    F[5] *= kSpi4;
-    F[6] *= kSpi4;
-    F[7] *= kSpi4;
+    c[5] = NSTATE == 3 ? -sb_max(sb_abs(SL), sb_abs(SR)) * dbx : 0.0f;
     if (!(sb_abs(SL) < 3.0e38f) || !(sb_abs(SR) < 3.0e38f)) flag |= kFlagStar;
+    return flag;
+}
+
+// Delta form on face states held in type D (FP64 in the delta form): side values rounded to
+// FP32, jumps formed in D then rounded, and the physical flux of the selected side in D.
+// kFlagStar also when NSTATE 2 sees a magnetic field (the delta form covers hydro HLLC only) --
+// the caller then recomputes the face in FP64.
+template <int NSTATE, typename D = double>
+SB_HD int riemann_delta(const D* q1, const D* q2, D* F, float& SLo, float& SRo, float& SMo) {
+    typedef float f;
+    const D ispi4 = D(kInvSpi4);
+    const D r1 = q1[0], u1 = q1[1], v1 = q1[2], w1 = q1[3], p1 = q1[4];
+    const D bx1 = q1[5] * ispi4, by1 = q1[6] * ispi4, bz1 = q1[7] * ispi4;
+    const D r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
+    const D bx2 = q2[5] * ispi4, by2 = q2[6] * ispi4, bz2 = q2[7] * ispi4;
+    const D b2L = (bx1 * bx1 + by1 * by1) + bz1 * bz1;
+    const D b2R = (bx2 * bx2 + by2 * by2) + bz2 * bz2;
+    const D ptL = p1 + D(0.5) * b2L, ptR = p2 + D(0.5) * b2R;
+    if (NSTATE == 2 && (b2L != D(0) || b2R != D(0))) return kFlagStar;
+    const D e1 = (p1 * D(kInvG1) + r1 * (D(0.5) * ((u1 * u1 + v1 * v1) + w1 * w1))) + D(0.5) * b2L;
+    const D e2 = (p2 * D(kInvG1) + r2 * (D(0.5) * ((u2 * u2 + v2 * v2) + w2 * w2))) + D(0.5) * b2R;
+    DeltaIn d;
+    d.r1 = (f)r1; d.u1 = (f)u1; d.v1 = (f)v1; d.w1 = (f)w1; d.p1 = (f)p1;
+    d.bx1 = (f)bx1; d.by1 = (f)by1; d.bz1 = (f)bz1; d.b2L = (f)b2L; d.e1 = (f)e1; d.ptL = (f)ptL;
+    d.r2 = (f)r2; d.u2 = (f)u2; d.v2 = (f)v2; d.w2 = (f)w2; d.p2 = (f)p2;
+    d.bx2 = (f)bx2; d.by2 = (f)by2; d.bz2 = (f)bz2; d.b2R = (f)b2R; d.e2 = (f)e2;
+    d.du = (f)(u2 - u1); d.dv = (f)(v2 - v1); d.dw = (f)(w2 - w1);
+    d.dbx = (f)(bx2 - bx1); d.dby = (f)(by2 - by1); d.dbz = (f)(bz2 - bz1);
+    d.dpt = (f)(ptR - ptL);
+    float c[8];
+    bool right;
+    const int flag = delta_core<NSTATE>(d, c, right, SLo, SRo, SMo);
+    // physical flux of the selected side
+    const D r = right ? r2 : r1, u = right ? u2 : u1, v = right ? v2 : v1, w = right ? w2 : w1;
+    const D bx = right ? bx2 : bx1, by = right ? by2 : by1, bz = right ? bz2 : bz1;
+    const D pt = right ? ptR : ptL, e = right ? e2 : e1;
+    const D m = r * u;
+    F[0] = m + (D)c[0];
+    F[1] = ((m * u + pt) - bx * bx) + (D)c[1];
+    F[2] = (m * v - bx * by) + (D)c[2];
+    F[3] = (m * w - bx * bz) + (D)c[3];
+    F[4] = ((e + pt) * u - bx * ((u * bx + v * by) + w * bz)) + (D)c[4];
+    F[5] = (D)c[5] * D(kSpi4);
+    F[6] = ((u * by - v * bx) + (D)c[6]) * D(kSpi4);
+    F[7] = ((u * bz - w * bx) + (D)c[7]) * D(kSpi4);
     return flag;
 }
 
