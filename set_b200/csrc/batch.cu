@@ -5,7 +5,7 @@
 //   compensation, a density snapshot for steady-state checks) allocated stream-ordered on the
 //   batch stream, so admitting or retiring a solve never synchronises the device.  Admission is
 //   by HBM footprint against a byte budget.
-// * A step is two persistent launches (Heun stages) whose CTAs draw 32x8xlz tiles of all active
+// * A step is two persistent launches (Heun stages) whose CTAs draw 32x7xlz tiles of all active
 //   solves from one work-queue counter; each solve counts its own tiles, so each keeps its own
 //   lagged dt and clock.  While membership is unchanged the launch sequence of a chunk of steps
 //   is replayed from a captured CUDA graph.
@@ -185,7 +185,7 @@ int rebuild(setb_batch* b) {
         Slot& sl = b->slots[s];
         GridGeom g = sl.g;
         g.lz = std::min(b->lz, g.nz);
-        const int ntx = (g.nx + 31) / 32, nty = (g.ny + 7) / 8, ntz = (g.nz + g.lz - 1) / g.lz;
+        const int ntx = (g.nx + kTileX - 1) / kTileX, nty = (g.ny + kTileY - 1) / kTileY, ntz = (g.nz + g.lz - 1) / g.lz;
         for (int bz = 0; bz < ntz; bz++)
             for (int by = 0; by < nty; by++)
                 for (int bx = 0; bx < ntx; bx++) items.push_back(make_int4(s, bx, by, bz));

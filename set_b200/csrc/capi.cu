@@ -100,7 +100,7 @@ GridGeom make_geom(const setb_cart_desc* d) {
 // z extent of one CTA's march: balances wave quantisation against the per-chunk prologue
 // (4 plane loads + 1 z face, costed as ~1.5 plane iterations).
 int choose_lz(const GridGeom& g, int sm_count, int ctas_per_sm) {
-    const long long cols = (long long)((g.nx + 31) / 32) * ((g.ny + 7) / 8);
+    const long long cols = (long long)((g.nx + kTileX - 1) / kTileX) * ((g.ny + kTileY - 1) / kTileY);
     const long long slots = (long long)sm_count * std::max(ctas_per_sm, 1);
     double best = 1e300;
     int best_lz = g.nz;

@@ -191,40 +191,38 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         SR = TR0;
     }
 
-    // left/right energies, fluxes and conserved vectors, :1368-1404
-    const T e1 = (p1 * ig1 + r1 * (half * ((u1 * u1 + v1 * v1) + w1 * w1))) + half * b2L;
-    const T e2 = (p2 * ig1 + r2 * (half * ((u2 * u2 + v2 * v2) + w2 * w2))) + half * b2R;
-    const T sbv1 = (u1 * bx1 + v1 * by1) + w1 * bz1;
-    const T sbv2 = (u2 * bx2 + v2 * by2) + w2 * bz2;
-    const T m1 = r1 * u1, m2 = r2 * u2;
-    T FL[8], FR[8], UL[8], UR[8];
-    FL[0] = m1;
-    FL[1] = (m1 * u1 + ptL) - bx1 * bx1;
-    FL[2] = m1 * v1 - bx1 * by1;
-    FL[3] = m1 * w1 - bx1 * bz1;
-    FL[4] = (e1 + ptL) * u1 - bx1 * sbv1;
-    FL[5] = T(0);
-    FL[6] = u1 * by1 - v1 * bx1;
-    FL[7] = u1 * bz1 - w1 * bx1;
-    FR[0] = m2;
-    FR[1] = (m2 * u2 + ptR) - bx2 * bx2;
-    FR[2] = m2 * v2 - bx2 * by2;
-    FR[3] = m2 * w2 - bx2 * bz2;
-    FR[4] = (e2 + ptR) * u2 - bx2 * sbv2;
-    FR[5] = T(0);
-    FR[6] = u2 * by2 - v2 * bx2;
-    FR[7] = u2 * bz2 - w2 * bx2;
-    UL[0] = r1; UL[1] = m1; UL[2] = r1 * v1; UL[3] = r1 * w1; UL[4] = e1;
-    UL[5] = bx1; UL[6] = by1; UL[7] = bz1;
-    UR[0] = r2; UR[1] = m2; UR[2] = r2 * v2; UR[3] = r2 * w2; UR[4] = e2;
-    UR[5] = bx2; UR[6] = by2; UR[7] = bz2;
-
     int flag = 0;
     const T isrl = sb_rcp(SR - SL);
     // HLL average of the normal field, UZ(6) (:1406-1408 with FL(6) = FR(6) = 0)
     const T bn = (SR * bx2 - SL * bx1) * isrl;
 
-    if (NSTATE <= 1) {   // :1414-1463
+    if (NSTATE <= 1) {   // :1414-1463, with the left/right energies, fluxes and states of :1368-1404
+        const T e1 = (p1 * ig1 + r1 * (half * ((u1 * u1 + v1 * v1) + w1 * w1))) + half * b2L;
+        const T e2 = (p2 * ig1 + r2 * (half * ((u2 * u2 + v2 * v2) + w2 * w2))) + half * b2R;
+        const T sbv1 = (u1 * bx1 + v1 * by1) + w1 * bz1;
+        const T sbv2 = (u2 * bx2 + v2 * by2) + w2 * bz2;
+        const T m1 = r1 * u1, m2 = r2 * u2;
+        T FL[8], FR[8], UL[8], UR[8];
+        FL[0] = m1;
+        FL[1] = (m1 * u1 + ptL) - bx1 * bx1;
+        FL[2] = m1 * v1 - bx1 * by1;
+        FL[3] = m1 * w1 - bx1 * bz1;
+        FL[4] = (e1 + ptL) * u1 - bx1 * sbv1;
+        FL[5] = T(0);
+        FL[6] = u1 * by1 - v1 * bx1;
+        FL[7] = u1 * bz1 - w1 * bx1;
+        FR[0] = m2;
+        FR[1] = (m2 * u2 + ptR) - bx2 * bx2;
+        FR[2] = m2 * v2 - bx2 * by2;
+        FR[3] = m2 * w2 - bx2 * bz2;
+        FR[4] = (e2 + ptR) * u2 - bx2 * sbv2;
+        FR[5] = T(0);
+        FR[6] = u2 * by2 - v2 * bx2;
+        FR[7] = u2 * bz2 - w2 * bx2;
+        UL[0] = r1; UL[1] = m1; UL[2] = r1 * v1; UL[3] = r1 * w1; UL[4] = e1;
+        UL[5] = bx1; UL[6] = by1; UL[7] = bz1;
+        UR[0] = r2; UR[1] = m2; UR[2] = r2 * v2; UR[3] = r2 * w2; UR[4] = e2;
+        UR[5] = bx2; UR[6] = by2; UR[7] = bz2;
         T TL = SL, TR = SR;
         if (SL > wv) TL = T(0);
         if (SR < wv) TR = T(0);
@@ -245,27 +243,34 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         }
         if (!(SL > wv) && !(SL <= wv && wv <= SR) && !(SR < wv)) flag |= kFlagWave;
     } else {
+        // The wave-fan region needs only SL, SR, SM and the star densities, so it is found first
+        // and the energy, physical flux and conserved vector (:1368-1404) and the star energy are
+        // formed for the selected side alone.
         const T isrm = sb_rcp(SR - SM), islm = sb_rcp(SL - SM);
         const T suRm = suR * isrm, suLm = suL * islm;
         const T rzR = r2 * suRm, rzL = r1 * suLm;
-        T vzL2, vzL3, vzR2, vzR3, bzL2, bzL3, bzR2, bzR3, ezL, ezR;
-        // selected-region coefficients: F = Fs + a2*(UZZs - UZs) + a1*(UZs - Us) - wv*Wsel
+        T vzL2, vzL3, vzR2, vzR3, bzL2, bzL3, bzR2, bzR3;
         int region;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
-        T vzz2 = T(0), vzz3 = T(0), bzz2 = T(0), bzz3 = T(0), ezzL = T(0), ezzR = T(0);
+        T vzz2 = T(0), vzz3 = T(0), bzz2 = T(0), bzz3 = T(0);
         T SZL = SM, SZR = SM;
-        T ptz;   // total pressure of the star states
+        T ptz;        // total pressure of the star states
+        T sbvz = T(0), rzRs = T(0), rzLs = T(0), sbn = T(0);
         bool ibn = false;
         if (NSTATE == 2) {   // HLLC, :1465-1567
             ptz = half * ((ptR + r2 * suR * (SM - u2)) + (ptL + r1 * suL * (SM - u1)));
-            const T uz0 = ((SR * r2 - SL * r1) + FL[0] - FR[0]) * isrl;
-            const T uz1 = ((SR * UR[1] - SL * UL[1]) + FL[1] - FR[1]) * isrl;
-            const T uz2 = ((SR * UR[2] - SL * UL[2]) + FL[2] - FR[2]) * isrl;
-            const T uz3 = ((SR * UR[3] - SL * UL[3]) + FL[3] - FR[3]) * isrl;
-            const T uz6 = ((SR * by2 - SL * by1) + FL[6] - FR[6]) * isrl;
-            const T uz7 = ((SR * bz2 - SL * bz1) + FL[7] - FR[7]) * isrl;
-            const T sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * sb_rcp(uz0);
-            ezR = e2 * suRm + (((ptz * SM - ptR * u2) + bn * (sbv2 - sbvz)) * isrm);
-            ezL = e1 * suLm + (((ptz * SM - ptL * u1) + bn * (sbv1 - sbvz)) * islm);
+            const T m1 = r1 * u1, m2 = r2 * u2;
+            const T FL1 = (m1 * u1 + ptL) - bx1 * bx1, FR1 = (m2 * u2 + ptR) - bx2 * bx2;
+            const T FL2 = m1 * v1 - bx1 * by1, FR2 = m2 * v2 - bx2 * by2;
+            const T FL3 = m1 * w1 - bx1 * bz1, FR3 = m2 * w2 - bx2 * bz2;
+            const T FL6 = u1 * by1 - v1 * bx1, FR6 = u2 * by2 - v2 * bx2;
+            const T FL7 = u1 * bz1 - w1 * bx1, FR7 = u2 * bz2 - w2 * bx2;
+            const T uz0 = ((SR * r2 - SL * r1) + m1 - m2) * isrl;
+            const T uz1 = ((SR * m2 - SL * m1) + FL1 - FR1) * isrl;
+            const T uz2 = ((SR * (r2 * v2) - SL * (r1 * v1)) + FL2 - FR2) * isrl;
+            const T uz3 = ((SR * (r2 * w2) - SL * (r1 * w1)) + FL3 - FR3) * isrl;
+            const T uz6 = ((SR * by2 - SL * by1) + FL6 - FR6) * isrl;
+            const T uz7 = ((SR * bz2 - SL * bz1) + FL7 - FR7) * isrl;
+            sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * sb_rcp(uz0);
             if (sb_abs(bn) < T(kEpsB)) {
                 vzR2 = v2; vzR3 = w2; vzL2 = v1; vzL3 = w1;
                 bzR2 = by2 * suRm; bzR3 = bz2 * suRm;
@@ -307,29 +312,16 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             bzL3 = bz1 * tbL;
             bzR2 = by2 * tbR;
             bzR3 = bz2 * tbR;
-            const T sbvL = (bn * SM + bzL2 * vzL2) + bzL3 * vzL3;
-            const T sbvR = (bn * SM + bzR2 * vzR2) + bzR3 * vzR3;
-            ezR = e2 * suRm + (((ptz * SM - ptR * u2) + bn * (sbv2 - sbvR)) * isrm);
-            ezL = e1 * suLm + (((ptz * SM - ptL * u1) + bn * (sbv1 - sbvL)) * islm);
             const T isR = sb_rsqrt(rzR), isL = sb_rsqrt(rzL);   // 1/sqrt(rho*) and sqrt(rho*) = rho*/sqrt(rho*)
-            const T rzRs = rzR * isR, rzLs = rzL * isL;
+            rzRs = rzR * isR;
+            rzLs = rzL * isL;
             const T abn = sb_abs(bn);
-            T sbn = T(0);
             if (abn > T(kEpsB)) {
                 ibn = true;
                 sbn = bn > T(0) ? T(1) : T(-1);
                 SZL = SM - abn * isL;
                 SZR = SM + abn * isR;
             }
-            const T irzss = sb_rcp(rzRs + rzLs);
-            const T rzps = rzRs * rzLs;
-            vzz2 = ((rzLs * vzL2 + rzRs * vzR2) + sbn * (bzR2 - bzL2)) * irzss;
-            vzz3 = ((rzLs * vzL3 + rzRs * vzR3) + sbn * (bzR3 - bzL3)) * irzss;
-            bzz2 = ((rzLs * bzR2 + rzRs * bzL2) + sbn * rzps * (vzR2 - vzL2)) * irzss;
-            bzz3 = ((rzLs * bzR3 + rzRs * bzL3) + sbn * rzps * (vzR3 - vzL3)) * irzss;
-            const T sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
-            ezzR = ezR + rzRs * sbn * (sbvR - sbzz);
-            ezzL = ezL - rzLs * sbn * (sbvL - sbzz);
             if (SR < wv) region = 6;
             else if (SZR <= wv && SR >= wv) region = 5;
             else if (ibn && SM <= wv && SZR >= wv) region = 4;
@@ -337,31 +329,64 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             else if (SL <= wv && SZL >= wv) region = 2;
             else if (SL > wv) region = 1;
             else region = 0;
+            if (region == 3 || region == 4) {
+                const T irzss = sb_rcp(rzRs + rzLs);
+                const T rzps = rzRs * rzLs;
+                vzz2 = ((rzLs * vzL2 + rzRs * vzR2) + sbn * (bzR2 - bzL2)) * irzss;
+                vzz3 = ((rzLs * vzL3 + rzRs * vzR3) + sbn * (bzR3 - bzL3)) * irzss;
+                bzz2 = ((rzLs * bzR2 + rzRs * bzL2) + sbn * rzps * (vzR2 - vzL2)) * irzss;
+                bzz3 = ((rzLs * bzR3 + rzRs * bzL3) + sbn * rzps * (vzR3 - vzL3)) * irzss;
+            }
         }
         if (region == 0) flag |= kFlagWave;
         const bool right = region >= 4;
-        // selected side (element-wise selects keep FL/FR/UL/UR in registers)
+        const bool use1 = (region == 2 || region == 3 || region == 4 || region == 5);
+        const bool use2 = (region == 3 || region == 4);
+        // the selected side
+        const T r = right ? r2 : r1, u = right ? u2 : u1, v = right ? v2 : v1, w = right ? w2 : w1;
+        const T p = right ? p2 : p1, bx = right ? bx2 : bx1, by = right ? by2 : by1, bz = right ? bz2 : bz1;
+        const T pt = right ? ptR : ptL, b2 = right ? b2R : b2L;
+        const T sum = right ? suRm : suLm, ism = right ? isrm : islm;
         const T rz = right ? rzR : rzL;
         const T S1 = right ? SR : SL;
         const T S2 = right ? SZR : SZL;
         const T vz2 = right ? vzR2 : vzL2, vz3 = right ? vzR3 : vzL3;
         const T bz2_ = right ? bzR2 : bzL2, bz3_ = right ? bzR3 : bzL3;
-        const T ez = right ? ezR : ezL, ezz = right ? ezzR : ezzL;
+        const T e = (p * ig1 + r * (half * ((u * u + v * v) + w * w))) + half * b2;
+        const T sbv = (u * bx + v * by) + w * bz;
+        const T m = r * u;
+        T Fs[8], Us[8];
+        Fs[0] = m;
+        Fs[1] = (m * u + pt) - bx * bx;
+        Fs[2] = m * v - bx * by;
+        Fs[3] = m * w - bx * bz;
+        Fs[4] = (e + pt) * u - bx * sbv;
+        Fs[5] = T(0);
+        Fs[6] = u * by - v * bx;
+        Fs[7] = u * bz - w * bx;
+        Us[0] = r; Us[1] = m; Us[2] = r * v; Us[3] = r * w; Us[4] = e;
+        Us[5] = bx; Us[6] = by; Us[7] = bz;
+        // star energy of the selected side (:1541-1544 / :1650-1656) and its double star
+        // (:1710-1718)
+        const T sbvS = NSTATE == 2 ? sbvz : (bn * SM + bz2_ * vz2) + bz3_ * vz3;
+        const T ez = e * sum + (((ptz * SM - pt * u) + bn * (sbv - sbvS)) * ism);
+        T ezz = ez;
+        if (NSTATE == 3 && use2) {
+            const T sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
+            ezz = right ? ez + rzRs * sbn * (sbvS - sbzz) : ez - rzLs * sbn * (sbvS - sbzz);
+        }
         T UZs[8], UZZs[8];
         UZs[0] = rz; UZs[1] = rz * SM; UZs[2] = rz * vz2; UZs[3] = rz * vz3; UZs[4] = ez;
         UZs[5] = bn; UZs[6] = bz2_; UZs[7] = bz3_;
         UZZs[0] = rz; UZZs[1] = rz * SM; UZZs[2] = rz * vzz2; UZZs[3] = rz * vzz3; UZZs[4] = ezz;
         UZZs[5] = bn; UZZs[6] = bzz2; UZZs[7] = bzz3;
-        const bool use1 = (region == 2 || region == 3 || region == 4 || region == 5);
-        const bool use2 = (region == 3 || region == 4);
         T W[8];   // the state whose flux is returned (for the face-speed term and the check)
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            const T us = right ? UR[k] : UL[k];
-            T f = right ? FR[k] : FL[k];
+            T f = Fs[k];
             if (use2) f = f + S2 * (UZZs[k] - UZs[k]);
-            if (use1) f = f + S1 * (UZs[k] - us);
-            W[k] = use2 ? UZZs[k] : (use1 ? UZs[k] : us);
+            if (use1) f = f + S1 * (UZs[k] - Us[k]);
+            W[k] = use2 ? UZZs[k] : (use1 ? UZs[k] : Us[k]);
             if (MOVING) f = f - wv * W[k];
             F[k] = f;
         }

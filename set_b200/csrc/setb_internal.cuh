@@ -10,6 +10,10 @@ namespace sb {
 // dev_time_all as device scalars written from the host each step (cuf_kernel.cuf:18-19,
 // 789-794); here the last CTA of each step's final kernel rolls the clock on the device, so a
 // run of steps needs no host round trip.
+// Column tile of the stage kernels: kTileX x kTileY cells marched along z by kStageThreads
+// threads (see stage.cu).
+constexpr int kTileX = 32, kTileY = 7, kStageThreads = 256;
+
 struct DevClock {
     double dt_cur;                  // dt used by the current step (time_step)
     unsigned long long dt_next;     // bits of the running min for the next step (time_step2)

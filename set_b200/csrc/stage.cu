@@ -4,7 +4,7 @@
 // CUF_MGD_cell_RK2, SET_Fortran_Cuda_MHD/cuf_solvers.cuf:243-440 and :561-794; Euler variants
 // :62-241, :443-558), which exchange fluxes through a 9 x N_gran array in HBM, with a single
 // kernel per stage:
-//   * a CTA owns a 32 x 8 column of cells and marches along z over lz planes;
+//   * a CTA owns a 32 x 7 column of cells and marches along z over lz planes;
 //   * each plane (cells + 2-cell x/y halo) is read from the SoA conserved state once, turned into
 //     primitives once (FP64 pressure recovery) and kept in a 4-plane shared-memory ring
 //     (planes k-1 .. k+2), which is all the z-stencil of the minmod reconstruction needs;
@@ -28,12 +28,15 @@
 namespace sb {
 namespace {
 
-// 32 x 8 cells per CTA, one thread per cell.  (288 threads would fit the 808 faces of a plane
-// into three rounds, but a sub-partition holding 3 of 9 warps caps FP64 HLLD at 168 registers
-// and spills.)
-constexpr int TX = 32, TY = 8, NT = TX * TY;
+// 32 x 7 cells per CTA and 256 threads: the 711 faces of a plane take three rounds of 256 (a
+// 32 x 8 tile has 808 faces, whose fourth round of 40 leaves 6 of 8 warps waiting at the
+// barrier; 288 threads would fit 808 faces into three rounds, but a sub-partition holding 3 of
+// 9 warps caps FP64 HLLD at 168 registers and spills).  Threads 0..223 own one cell each in the
+// update.
+constexpr int TX = kTileX, TY = kTileY, NC = TX * TY, NT = kStageThreads;
+static_assert(NC <= NT, "one thread per cell in the update");
 constexpr int HX = TX + 4, HY = TY + 4, PLANE = HX * HY;
-constexpr int NZF = NT;                   // z faces k+1/2 of the column tile
+constexpr int NZF = NC;                   // z faces k+1/2 of the column tile
 constexpr int NXF = (TX + 1) * TY;        // x faces
 constexpr int NYF = TX * (TY + 1);        // y faces
 constexpr int NF = NZF + NXF + NYF;
@@ -96,7 +99,7 @@ __device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j
     return fl;
 }
 
-// One tile of one stage: the column (bx, by) of 32 x 8 cells, planes [bz*lz, min(nz, (bz+1)*lz)).
+// One tile of one stage: the column (bx, by) of TX x TY cells, planes [bz*lz, min(nz, (bz+1)*lz)).
 // `total_tiles` is the number of tiles of this solve in the launch; the last one to finish rolls
 // the solve's clock.  Called by the single-solve kernel (one tile per CTA) and by the batch
 // kernel (tiles of many solves drawn from a work queue); every CTA-wide barrier is reached by all
@@ -276,7 +279,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     for (int kk = k0 - 2; kk <= k0; kk++) load_plane<RG>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
     double fzl[8];
     const int gi = i0 + tx, gj = j0 + ty;
-    const bool own = (gi < g.nx) && (gj < g.ny);
+    const bool own = (t < NC) && (gi < g.nx) && (gj < g.ny);
     for (int k = k0 - 1; k < k1; k++) {
         load_plane<RG>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
         __syncthreads();
@@ -286,7 +289,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         __syncthreads();
         double fzh[8];
 #pragma unroll
-        for (int v = 0; v < 8; v++) fzh[v] = (double)fz[v * NZF + t];
+        for (int v = 0; v < 8; v++) fzh[v] = t < NC ? (double)fz[v * NZF + t] : 0.0;
         if (pro) {
 #pragma unroll
             for (int v = 0; v < 8; v++) fzl[v] = fzh[v];

@@ -1,9 +1,9 @@
 """Batched solves (setb_batch_*): per-solve results independent of the batch.
 
 * A solve in a batch matches the same solve run alone through the single-solve handle: plain
-  FP64 relative L1 <= 1e-12 per conserved variable; mixed <= 1e-6, the mixed form's accuracy class
-  (the same tile arithmetic compiled into a different kernel contracts FP32 operations
-  differently; measured 4.5e-8).
+  FP64 relative L1 <= 1e-12 per conserved variable (vector components against the vector's
+  L1); mixed <= 1e-6, the mixed form's accuracy class (the same tile arithmetic compiled into a
+  different kernel contracts FP32 operations differently).
 * A solve alone in a batch and the same solve in a mix (with members added and removed between
   steps) are bit-identical, and so are their steady-state check values.
 """
@@ -15,8 +15,18 @@ import set_b200 as S
 pytestmark = pytest.mark.gpu
 
 
+def l1_vars(a, b):
+    """Relative L1 per conserved variable; momentum and B components are measured against the
+    whole vector's L1 (a component that is near zero everywhere has no scale of its own)."""
+    d = np.abs(a - b).reshape(8, -1).sum(1)
+    s = np.abs(b).reshape(8, -1).sum(1)
+    s[1:4] = s[1:4].sum()
+    s[5:8] = s[5:8].sum()
+    return d / np.maximum(s, 1e-300)
+
+
 def l1(a, b):
-    return (np.abs(a - b).reshape(8, -1).sum(1) / np.maximum(np.abs(b).reshape(8, -1).sum(1), 1e-300)).max()
+    return l1_vars(a, b).max()
 
 
 PROBLEMS = [
@@ -49,7 +59,7 @@ def test_batch_matches_single_solves(precision):
         with S.Solver(d, ic=ic) as s:
             t = s.step(25, o)
             ref = s.conserved()
-        assert l1(got[k], ref) <= tol, (k, l1(got[k], ref))
+        assert l1(got[k], ref) <= tol, (k, l1_vars(got[k], ref))
         assert abs(stat[k].time_all - t) <= tol * t and stat[k].steps == 25
 
 
