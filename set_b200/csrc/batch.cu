@@ -185,7 +185,8 @@ int rebuild(setb_batch* b) {
         Slot& sl = b->slots[s];
         GridGeom g = sl.g;
         g.lz = std::min(b->lz, g.nz);
-        const int ntx = (g.nx + kTileX - 1) / kTileX, nty = (g.ny + kTileY - 1) / kTileY, ntz = (g.nz + g.lz - 1) / g.lz;
+        const int ty = tile_shape(b->precision).ty;
+        const int ntx = (g.nx + kTileX - 1) / kTileX, nty = (g.ny + ty - 1) / ty, ntz = (g.nz + g.lz - 1) / g.lz;
         for (int bz = 0; bz < ntz; bz++)
             for (int by = 0; by < nty; by++)
                 for (int bx = 0; bx < ntx; bx++) items.push_back(make_int4(s, bx, by, bz));

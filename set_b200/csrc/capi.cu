@@ -99,9 +99,10 @@ GridGeom make_geom(const setb_cart_desc* d) {
 
 // z extent of one CTA's march: balances wave quantisation against the per-chunk prologue
 // (4 plane loads + 1 z face, costed as ~1.5 plane iterations).
-int choose_lz(const GridGeom& g, int sm_count, int ctas_per_sm) {
-    const long long cols = (long long)((g.nx + kTileX - 1) / kTileX) * ((g.ny + kTileY - 1) / kTileY);
-    const long long slots = (long long)sm_count * std::max(ctas_per_sm, 1);
+int choose_lz(const GridGeom& g, int sm_count, int precision) {
+    const TileShape ts = tile_shape(precision);
+    const long long cols = (long long)((g.nx + kTileX - 1) / kTileX) * ((g.ny + ts.ty - 1) / ts.ty);
+    const long long slots = (long long)sm_count * std::max(ts.ctas_per_sm, 1);
     double best = 1e300;
     int best_lz = g.nz;
     for (int c = 1; c <= std::max(1, g.nz / 8); c++) {
@@ -190,8 +191,8 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
         return SETB_ECUDA;
     }
     h->sm_count = prop.multiProcessorCount;
-    h->ctas_per_sm = 1;   // plain form: 256 threads x up to 255 registers; the mixed form runs 2
-    h->g.lz = choose_lz(h->g, h->sm_count, h->ctas_per_sm);
+    h->ctas_per_sm = tile_shape(0).ctas_per_sm;
+    h->g.lz = choose_lz(h->g, h->sm_count, 0);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
         return SETB_ECUDA;
@@ -380,7 +381,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     StageArgs a{};
     a.g = h->g;
     const int P = o->precision;
-    a.g.lz = choose_lz(h->g, h->sm_count, batch_ctas_per_sm(P));
+    a.g.lz = choose_lz(h->g, h->sm_count, P);
     float* comp = nullptr;
     if (P != 0) {
         if (!h->comp) {

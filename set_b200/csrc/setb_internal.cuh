@@ -10,9 +10,17 @@ namespace sb {
 // dev_time_all as device scalars written from the host each step (cuf_kernel.cuf:18-19,
 // 789-794); here the last CTA of each step's final kernel rolls the clock on the device, so a
 // run of steps needs no host round trip.
-// Column tile of the stage kernels: kTileX x kTileY cells marched along z by kStageThreads
-// threads (see stage.cu).
-constexpr int kTileX = 32, kTileY = 7, kStageThreads = 256;
+// Column tile of the stage kernels: kTileX x ty cells marched along z by `threads` threads,
+// `ctas_per_sm` resident per SM; per form (precision 0 plain FP64, 1 mixed, 2 delta).  The
+// plain and delta forms fit FP64 HLLD in 168 registers (384 threads, 12 warps per SM); the mixed
+// form runs two 256-thread CTAs of at most 128 registers.
+constexpr int kTileX = 32;
+struct TileShape {
+    int ty, threads, ctas_per_sm;
+};
+SB_HD constexpr TileShape tile_shape(int precision) {
+    return precision == 1 ? TileShape{7, 256, 2} : TileShape{11, 384, 1};
+}
 
 struct DevClock {
     double dt_cur;                  // dt used by the current step (time_step)

@@ -4,13 +4,14 @@
 // CUF_MGD_cell_RK2, SET_Fortran_Cuda_MHD/cuf_solvers.cuf:243-440 and :561-794; Euler variants
 // :62-241, :443-558), which exchange fluxes through a 9 x N_gran array in HBM, with a single
 // kernel per stage:
-//   * a CTA owns a 32 x 7 column of cells and marches along z over lz planes;
+//   * a CTA owns a 32 x TY column of cells and marches along z over lz planes;
 //   * each plane (cells + 2-cell x/y halo) is read from the SoA conserved state once, turned into
 //     primitives once (FP64 pressure recovery) and kept in a 4-plane shared-memory ring
 //     (planes k-1 .. k+2), which is all the z-stencil of the minmod reconstruction needs;
 //   * every face of the plane (x, y and the z face k+1/2) is computed once, by one thread, from
 //     shared memory, and its flux is applied to both neighbouring cells (the z face k-1/2 is
-//     carried in registers from the previous plane);
+//     carried in registers from the previous plane); faces are handed out in warp-sized jobs of
+//     one axis, so the face-frame permutation is a compile-time constant;
 //   * the conservative update, p floor, source re-imposition and the dt candidate reduction
 //     (warp shuffle -> one atomicMin per CTA) are fused; the last CTA rolls the lagged-dt clock.
 //
@@ -21,6 +22,7 @@
 //   the FP64 state; the flux divergence and the update are FP64, and the second Heun stage (or
 //   the Euler step) is a compensated sum with the compensation kept in FP32; dt is reduced in
 //   FP64.  Half the shared memory and at most 128 registers give two CTAs per SM.
+// P = 2, delta form: FP64 ring and fluxes, the Riemann solver's small differences in FP32.
 #include <cfloat>
 #include <type_traits>
 #include "setb_internal.cuh"
@@ -28,18 +30,20 @@
 namespace sb {
 namespace {
 
-// 32 x 7 cells per CTA and 256 threads: the 711 faces of a plane take three rounds of 256 (a
-// 32 x 8 tile has 808 faces, whose fourth round of 40 leaves 6 of 8 warps waiting at the
-// barrier; 288 threads would fit 808 faces into three rounds, but a sub-partition holding 3 of
-// 9 warps caps FP64 HLLD at 168 registers and spills).  Threads 0..223 own one cell each in the
-// update.
-constexpr int TX = kTileX, TY = kTileY, NC = TX * TY, NT = kStageThreads;
-static_assert(NC <= NT, "one thread per cell in the update");
-constexpr int HX = TX + 4, HY = TY + 4, PLANE = HX * HY;
-constexpr int NZF = NC;                   // z faces k+1/2 of the column tile
-constexpr int NXF = (TX + 1) * TY;        // x faces
-constexpr int NYF = TX * (TY + 1);        // y faces
-constexpr int NF = NZF + NXF + NYF;
+// Column tile of each form (tile_shape): TX = 32 cells per tile row, one lane per column.  The
+// 3 TY + 2 warp jobs of a plane's faces (see run_tile) take three rounds of the CTA's warps
+// (32 x 7 cells: 23 jobs over 8 warps; 32 x 11: 35 jobs over 12 warps).  Threads 0..NC-1 own
+// one cell each in the update.
+template <int P> struct Tile {
+    static constexpr int TX = kTileX, TY = tile_shape(P).ty, NT = tile_shape(P).threads;
+    static constexpr int MINB = tile_shape(P).ctas_per_sm;
+    static constexpr int NC = TX * TY;
+    static constexpr int HX = TX + 4, HY = TY + 4, PLANE = HX * HY;
+    static constexpr int NXF = (TX + 1) * TY;        // x faces
+    static constexpr int NYF = TX * (TY + 1);        // y faces
+    static_assert(TX == 32, "one lane per tile column");
+    static_assert(NC <= NT, "one thread per cell in the update");
+};
 constexpr int RING = 4;
 
 __device__ __forceinline__ int ring_slot(int k) { return (k + 4 * RING) & (RING - 1); }
@@ -65,8 +69,9 @@ __device__ __forceinline__ void fetch_prim64(const StageArgs& A, int i, int j, i
 }
 
 // Loads plane kk (with halo) of the tile starting at (i0, j0) as primitives into `dst`.
-template <typename RT>
+template <int P, typename RT>
 __device__ __forceinline__ void load_plane(const StageArgs& A, RT* dst, int i0, int j0, int kk) {
+    constexpr int HX = Tile<P>::HX, PLANE = Tile<P>::PLANE, NT = Tile<P>::NT;
     for (int c = threadIdx.x; c < PLANE; c += NT) {
         const int cx = c % HX, cy = c / HX;
         double q[8];
@@ -74,6 +79,35 @@ __device__ __forceinline__ void load_plane(const StageArgs& A, RT* dst, int i0, 
 #pragma unroll
         for (int v = 0; v < 8; v++) dst[v * PLANE + c] = (RT)q[v];
     }
+}
+
+// Face-frame order (normal, t1, t2) of the components of a face normal to axis AX: entry v of
+// the face-frame state is natural component face_perm<AX>(v) of (rho, u, v, w, p, Bx, By, Bz).
+template <int AX> __host__ __device__ constexpr int face_perm(int v) {
+    return (v == 0 || v == 4) ? v
+           : (v < 4 ? 0 : 4) + ((v & 3) == 1 ? 1 + AX : ((v & 3) == 2 ? (AX == 0 ? 2 : 1) : (AX == 2 ? 2 : 3)));
+}
+
+// Face-frame states of the 4-cell stencil of a face normal to AX, from ring cells (component
+// planes PLANE apart).  B is first order, so only the inner pair carries it.
+template <int AX, int PLANE, typename RG, typename RT>
+__device__ __forceinline__ void gather_face(const RG* pLL, const RG* pL, const RG* pR, const RG* pRR, RT* qLL,
+                                            RT* qL, RT* qR, RT* qRR) {
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        const int o = face_perm<AX>(v) * PLANE;
+        qL[v] = (RT)pL[o];
+        qR[v] = (RT)pR[o];
+        qLL[v] = v < 5 ? (RT)pLL[o] : RT(0);
+        qRR[v] = v < 5 ? (RT)pRR[o] : RT(0);
+    }
+}
+
+// Face-frame flux times the face area into natural component order, components STRIDE apart.
+template <int AX, int STRIDE, typename FT, typename RT>
+__device__ __forceinline__ void scatter_face(FT* out, const RT* F, RT sq) {
+#pragma unroll
+    for (int v = 0; v < 8; v++) out[face_perm<AX>(v) * STRIDE] = (FT)(F[v] * sq);
 }
 
 // The FP64 recompute of one face of the mixed form (rare path; kept out of line so the FP32
@@ -116,16 +150,8 @@ template <> struct Types<2> {   // delta form: FP64 states and fluxes, FP32 insi
     using Math = double;
 };
 template <> struct Types<1> {
-#if defined(SB_MIXED_RING_FP64)
-    using Ring = double;
-#else
     using Ring = float;
-#endif
-#if defined(SB_MIXED_FLUX_FP64)
-    using Flux = double;
-#else
     using Flux = float;
-#endif
     using Math = float;
 };
 
@@ -143,10 +169,12 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     using RG = typename Types<P>::Ring;
     using FT = typename Types<P>::Flux;
     using RT = typename Types<P>::Math;
+    using C = Tile<P>;
+    constexpr int TX = C::TX, TY = C::TY, NC = C::NC, NT = C::NT, HX = C::HX, PLANE = C::PLANE;
+    constexpr int NXF = C::NXF, NYF = C::NYF;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RG* ring = reinterpret_cast<RG*>(smem_raw);
-    FT* fz = reinterpret_cast<FT*>(ring + RING * 8 * PLANE);   // [8][NZF]
-    FT* fx = fz + 8 * NZF;                                      // [8][NXF]
+    FT* fx = reinterpret_cast<FT*>(ring + RING * 8 * PLANE);   // [8][NXF]
     FT* fy = fx + 8 * NXF;                                      // [8][NYF]
     __shared__ double red[NT / 32];
     __shared__ unsigned long long cnt[5];
@@ -164,75 +192,73 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     double rate = 0.0;   // max over this thread's real faces of max(|SL|,|SR|)/dist
     unsigned n_recon = 0, n_wave = 0, n_redo = 0;
 
-    // Computes face f of plane k (flattened: z faces, x faces, y faces) into fz/fx/fy.
+    // Faces are handed out in warp-sized jobs, so the face axis is uniform across a warp and the
+    // face-frame permutation of the components is a compile-time constant of the gather and the
+    // scatter (face_perm):
+    //   jobs [0, TY)         z faces k+1/2 of tile row `job`, column = lane;
+    //   jobs [TY, 2TY)       x faces i-1/2 of tile row `job - TY`, column = lane;
+    //   job  2TY             the east x faces (column TX) of tile rows 0 .. TY-1, row = lane;
+    //   jobs [2TY+1, 3TY+2)  y faces j-1/2 of tile row `job - 2TY - 1` (TY+1 rows), column = lane.
+    // Warp w runs jobs w, w + NW, ...; z job w (round 0) is run by the threads owning the cells of
+    // tile row w in the update.  A z flux goes into the ring slot of plane k-1 at its column:
+    // only the same thread reads that location in this plane (as the z face's far-left cell), and
+    // it reads the flux back before the barrier that precedes the next plane load.  x and y
+    // fluxes go to fx / fy.
     // `dup`: the face is also computed by the CTA below (chunk-boundary z face); it still enters
     // the dt candidate (min is idempotent) but not the diagnostic counters.
-    auto do_face = [&](int f, int k, bool dup) {
-        int axis, cLL, cL, cR, cRR, fxx, fyy, gk;
-        const RG *sLL, *sL, *sR, *sRR;
+    static_assert(std::is_same<RG, FT>::value, "z fluxes reuse the ring");
+    constexpr int NW = NT / 32;
+    constexpr int JZ = TY, JX = 2 * TY + 1, JOBS = 3 * TY + 2;
+    static_assert(TY <= NW, "z jobs run in the first round, by the owners of their cells");
+    const int lane = t & 31, warp = t >> 5;
+    auto do_face = [&](int job, int k, bool dup) {
+        int axis, fxx, fyy, gk, oidx, ostride;
         FT* out;
-        int oidx, ostride;
         bool real;
-        if (f < NZF) {
-            fxx = f % TX;
-            fyy = f / TX;
+        RT qLL[8], qL[8], qR[8], qRR[8];
+        if (job < JZ) {
             axis = 2;
+            fxx = lane;
+            fyy = job;
             const int c = (fyy + 2) * HX + fxx + 2;
-            cLL = cL = cR = cRR = c;
-            sLL = ring + ring_slot(k - 1) * 8 * PLANE;
-            sL = ring + ring_slot(k) * 8 * PLANE;
-            sR = ring + ring_slot(k + 1) * 8 * PLANE;
-            sRR = ring + ring_slot(k + 2) * 8 * PLANE;
-            out = fz;
-            oidx = f;
-            ostride = NZF;
+            gather_face<2, PLANE>(ring + ring_slot(k - 1) * 8 * PLANE + c, ring + ring_slot(k) * 8 * PLANE + c,
+                                  ring + ring_slot(k + 1) * 8 * PLANE + c, ring + ring_slot(k + 2) * 8 * PLANE + c,
+                                  qLL, qL, qR, qRR);
+            out = ring + ring_slot(k - 1) * 8 * PLANE;
+            oidx = c;
+            ostride = PLANE;
             gk = k + 1;
             real = (i0 + fxx < g.nx) && (j0 + fyy < g.ny) && (k + 1 <= g.nz) && (k + 1 >= 0);
-        } else if (f < NZF + NXF) {
-            const int idx = f - NZF;
-            fyy = idx / (TX + 1);
-            fxx = idx % (TX + 1);
+        } else if (job < JX) {
             axis = 0;
+            if (job < 2 * TY) {
+                fxx = lane;
+                fyy = job - JZ;
+            } else {
+                if (lane >= TY) return;
+                fxx = TX;
+                fyy = lane;
+            }
             const int c = (fyy + 2) * HX + fxx;   // cell fxx-2 (tile-local) at halo offset +2
-            cLL = c; cL = c + 1; cR = c + 2; cRR = c + 3;
-            sLL = sL = sR = sRR = ring + ring_slot(k) * 8 * PLANE;
+            const RG* b = ring + ring_slot(k) * 8 * PLANE + c;
+            gather_face<0, PLANE>(b, b + 1, b + 2, b + 3, qLL, qL, qR, qRR);
             out = fx;
-            oidx = idx;
+            oidx = fyy * (TX + 1) + fxx;
             ostride = NXF;
             gk = k;
             real = (i0 + fxx <= g.nx) && (j0 + fyy < g.ny);
         } else {
-            const int idx = f - NZF - NXF;
-            fyy = idx / TX;
-            fxx = idx % TX;
             axis = 1;
+            fxx = lane;
+            fyy = job - JX;
             const int c = fyy * HX + fxx + 2;     // row fyy-2 (tile-local)
-            cLL = c; cL = c + HX; cR = c + 2 * HX; cRR = c + 3 * HX;
-            sLL = sL = sR = sRR = ring + ring_slot(k) * 8 * PLANE;
+            const RG* b = ring + ring_slot(k) * 8 * PLANE + c;
+            gather_face<1, PLANE>(b, b + HX, b + 2 * HX, b + 3 * HX, qLL, qL, qR, qRR);
             out = fy;
-            oidx = idx;
+            oidx = fyy * TX + fxx;
             ostride = NYF;
             gk = k;
             real = (i0 + fxx < g.nx) && (j0 + fyy <= g.ny);
-        }
-        // face-frame permutation of the velocity / B components
-        const int pn = 1 + axis;
-        const int pt1 = axis == 0 ? 2 : 1;
-        const int pt2 = axis == 2 ? 2 : 3;
-        RT qLL[8], qL[8], qR[8], qRR[8];
-        const int perm[8] = {0, pn, pt1, pt2, 4, 4 + pn, 4 + pt1, 4 + pt2};
-#pragma unroll
-        for (int v = 0; v < 8; v++) {
-            const int o = perm[v] * PLANE;
-            qL[v] = (RT)sL[o + cL];
-            qR[v] = (RT)sR[o + cR];
-            if (v < 5) {
-                qLL[v] = (RT)sLL[o + cLL];
-                qRR[v] = (RT)sRR[o + cRR];
-            } else {
-                qLL[v] = RT(0);
-                qRR[v] = RT(0);
-            }
         }
         RT q1[8], q2[8], F[8];
         reconstruct<RT, ORDER>(qLL, qL, qR, qRR, q1, q2);
@@ -266,8 +292,9 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 #pragma unroll
                 for (int v = 0; v < 8; v++) F[v] = RT(0);
             }
-#pragma unroll
-            for (int v = 0; v < 8; v++) out[perm[v] * ostride + oidx] = (FT)(F[v] * (RT)sq);
+            if (axis == 2) scatter_face<2, PLANE>(out + oidx, F, (RT)sq);
+            else if (axis == 0) scatter_face<0, NXF>(out + oidx, F, (RT)sq);
+            else scatter_face<1, NYF>(out + oidx, F, (RT)sq);
         }
         if ((fl & kFlagWave) && real && !dup) n_wave++;
         if (WANT_DT && real) rate = fmax(rate, fmax(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
@@ -276,20 +303,23 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     // ---- the march.  Iteration k0-1 is the prologue: planes k0-2 .. k0+1 and only the z face
     // k0-1/2 (carried into the first update).  Every face goes through the one do_face call
     // site below, so a face's arithmetic does not depend on where a chunk starts.
-    for (int kk = k0 - 2; kk <= k0; kk++) load_plane<RG>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
+    for (int kk = k0 - 2; kk <= k0; kk++) load_plane<P, RG>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
     double fzl[8];
     const int gi = i0 + tx, gj = j0 + ty;
     const bool own = (t < NC) && (gi < g.nx) && (gj < g.ny);
     for (int k = k0 - 1; k < k1; k++) {
-        load_plane<RG>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
+        load_plane<P, RG>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
         __syncthreads();
         const bool pro = (k < k0);
-        const int nf = pro ? NZF : NF;
-        for (int f = t; f < nf; f += NT) do_face(f, k, pro && k0 > 0);
-        __syncthreads();
+        const int njobs = pro ? JZ : JOBS;
+        for (int job = warp; job < njobs; job += NW) do_face(job, k, pro && k0 > 0);
         double fzh[8];
+        {
+            const RG* zk = ring + ring_slot(k - 1) * 8 * PLANE + (ty + 2) * HX + tx + 2;
 #pragma unroll
-        for (int v = 0; v < 8; v++) fzh[v] = t < NC ? (double)fz[v * NZF + t] : 0.0;
+            for (int v = 0; v < 8; v++) fzh[v] = t < NC ? (double)zk[v * PLANE] : 0.0;
+        }
+        __syncthreads();
         if (pro) {
 #pragma unroll
             for (int v = 0; v < 8; v++) fzl[v] = fzh[v];
@@ -406,7 +436,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) stage_kernel(const StageArgs A) {
+__global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) stage_kernel(const StageArgs A) {
     run_tile<P, NSTATE, ORDER, KIND, WANT_DT>(A, blockIdx.x, blockIdx.y, blockIdx.z,
                                                gridDim.x * gridDim.y * gridDim.z);
 }
@@ -415,7 +445,7 @@ __global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) stage_kernel(const StageAr
 // tile's solve selects the arguments (copied to shared memory) and the Riemann solver.  The
 // items of one solve are counted by its own clock, so every solve keeps its own lagged dt.
 template <int P, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) batch_stage_kernel(const BatchArgs B) {
+__global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) batch_stage_kernel(const BatchArgs B) {
     __shared__ __align__(16) StageArgs As;
     __shared__ int4 it;
     constexpr int WORDS = sizeof(StageArgs) / sizeof(unsigned long long);
@@ -430,7 +460,7 @@ __global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) batch_stage_kernel(const B
         if (w.x < 0) break;
         const unsigned long long* src = reinterpret_cast<const unsigned long long*>(B.inst + w.x);
         unsigned long long* dst = reinterpret_cast<unsigned long long*>(&As);
-        for (int q = threadIdx.x; q < WORDS; q += NT) dst[q] = src[q];
+        for (int q = threadIdx.x; q < WORDS; q += Tile<P>::NT) dst[q] = src[q];
         __syncthreads();
         if (As.n_state == 3)
             run_tile<P, 3, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles);
@@ -441,8 +471,8 @@ __global__ void __launch_bounds__(NT, P == 1 ? 2 : 1) batch_stage_kernel(const B
 
 template <int P>
 constexpr int smem_bytes() {
-    return RING * 8 * PLANE * (int)sizeof(typename Types<P>::Ring) +
-           8 * (NZF + NXF + NYF) * (int)sizeof(typename Types<P>::Flux);
+    return RING * 8 * Tile<P>::PLANE * (int)sizeof(typename Types<P>::Ring) +
+           8 * (Tile<P>::NXF + Tile<P>::NYF) * (int)sizeof(typename Types<P>::Flux);
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
@@ -455,8 +485,9 @@ cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
+    constexpr int TX = Tile<P>::TX, TY = Tile<P>::TY;
     dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, (a.g.nz + a.g.lz - 1) / a.g.lz);
-    kern<<<grid, NT, smem, s>>>(a);
+    kern<<<grid, Tile<P>::NT, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -502,10 +533,11 @@ cudaError_t prepare_batch_kernels(int precision) {
     return batch_attr<0, 1, false>();
 }
 
-int batch_ctas_per_sm(int precision) { return precision == 1 ? 2 : 1; }
+int batch_ctas_per_sm(int precision) { return tile_shape(precision).ctas_per_sm; }
 
 template <int P>
 void launch_batch_p(const BatchArgs& b, int kind, bool want_dt, int grid, cudaStream_t s) {
+    constexpr int NT = Tile<P>::NT;
     if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P>(), s>>>(b);
     else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P>(), s>>>(b);
 }
