@@ -43,6 +43,7 @@ struct Slot {
     double* rho_prev = nullptr;
     DevClock* clk = nullptr;
     DevStatus* st = nullptr;
+    CUtensorMap* tmap = nullptr;   // [U, W] for the batch's tile shape
     long long steps = 0;
     bool have_prev = false;
 };
@@ -131,9 +132,10 @@ namespace {
         if (e_ != cudaSuccess) return SETB_ECUDA; \
     } while (0)
 
+// U, W, rho_prev, compensation, then clock (256 B), counters (256 B) and two tensor maps.
 size_t slot_bytes(const GridGeom& g) {
     return 2 * sizeof(double) * 8 * (size_t)g.vs + sizeof(float) * 8 * (size_t)g.vs + sizeof(double) * (size_t)g.vs +
-           512;
+           512 + 2 * sizeof(CUtensorMap);
 }
 
 GridGeom geom_of(const setb_cart_desc* d) {
@@ -141,9 +143,7 @@ GridGeom geom_of(const setb_cart_desc* d) {
     g.nx = d->nx;
     g.ny = d->ny;
     g.nz = d->nz;
-    g.px = d->nx;
-    g.ps = (long long)d->nx * d->ny;
-    g.vs = (g.ps * d->nz + 31) / 32 * 32;
+    set_device_strides(g);
     const int n[3] = {d->nx, d->ny, d->nz};
     for (int a = 0; a < 3; a++) {
         g.lo[a] = d->lo[a];
@@ -201,12 +201,14 @@ int rebuild(setb_batch* b) {
             a.total_tiles = (unsigned)(ntx * nty * ntz);
             if (st == 0) {
                 a.Uin = sl.U;
+                a.tm_in = sl.tmap;
                 a.Ubase = nullptr;
                 a.Uout = sl.W;
                 a.finalize = 0;
                 a.comp = nullptr;
             } else {
                 a.Uin = sl.W;
+                a.tm_in = sl.tmap ? sl.tmap + 1 : nullptr;
                 a.Ubase = sl.U;
                 a.Uout = sl.U;
                 a.finalize = 1;
@@ -377,6 +379,12 @@ int32_t setb_batch_add(setb_batch* b, const setb_cart_desc* d, const setb_lism_i
     p += sizeof(float) * 8 * vs;
     sl.clk = reinterpret_cast<DevClock*>(p);
     sl.st = reinterpret_cast<DevStatus*>(p + 256);
+    sl.tmap = reinterpret_cast<CUtensorMap*>(p + 512);
+    CUtensorMap tm[2] = {};
+    if (encode_state_tmap(sl.g, sl.U, b->precision, &tm[0]) != SETB_OK ||
+        encode_state_tmap(sl.g, sl.W, b->precision, &tm[1]) != SETB_OK) {
+        sl.tmap = nullptr;   // plain loads for this solve
+    }
     // initial condition, clock, counters, compensation (all stream-ordered, no host sync)
     double* dl = sl.W;   // 8 doubles of scratch for the LISM vector
     DevClock c{};
@@ -387,8 +395,10 @@ int32_t setb_batch_add(setb_batch* b, const setb_cart_desc* d, const setb_lism_i
     st.first_bad = ULLONG_MAX;
     SB_TRY(cudaStreamSynchronize(b->stream));   // the pinned staging area is reused below
     std::memcpy(b->h_check, ic->lism, sizeof(double) * 8);   // h_check holds >= 8 doubles
+    SB_TRY(cudaMemsetAsync(sl.U, 0, sizeof(double) * 8 * vs, b->stream));   // zero row padding
     SB_TRY(cudaMemcpyAsync(dl, b->h_check, sizeof(double) * 8, cudaMemcpyHostToDevice, b->stream));
     SB_TRY(launch_lism_init(sl.g, dl, ic->seed, ic->pert_amp, sl.U, b->stream));
+    if (sl.tmap) SB_TRY(cudaMemcpyAsync(sl.tmap, tm, sizeof(tm), cudaMemcpyHostToDevice, b->stream));
     SB_TRY(cudaMemcpyAsync(sl.clk, &c, sizeof(c), cudaMemcpyHostToDevice, b->stream));
     SB_TRY(cudaMemcpyAsync(sl.st, &st, sizeof(st), cudaMemcpyHostToDevice, b->stream));
     SB_TRY(cudaMemsetAsync(sl.comp, 0, sizeof(float) * 8 * vs, b->stream));
@@ -439,7 +449,7 @@ int32_t setb_batch_check(setb_batch* b, double* rel_change) {
         Slot& sl = b->slots[idx[q]];
         hr[q] = sl.U;   // density plane of U^n
         hp[q] = sl.rho_prev;
-        hn[q] = (long long)sl.g.nx * sl.g.ny * sl.g.nz;
+        hn[q] = sl.g.ps * sl.g.nz;   // row padding holds zeros in U and in rho_prev
     }
     SB_TRY(cudaMemcpyAsync(b->d_rho, hr, sizeof(double*) * n, cudaMemcpyHostToDevice, b->stream));
     SB_TRY(cudaMemcpyAsync(b->d_prev, hp, sizeof(double*) * n, cudaMemcpyHostToDevice, b->stream));
@@ -463,7 +473,9 @@ int32_t setb_batch_get_conserved(setb_batch* b, int32_t slot, double* U) {
     const Slot& sl = b->slots[slot];
     const size_t N = (size_t)sl.g.nx * sl.g.ny * sl.g.nz;
     for (int v = 0; v < 8; v++)
-        SB_TRY(cudaMemcpyAsync(U + v * N, sl.U + v * sl.g.vs, N * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+        SB_TRY(cudaMemcpy2DAsync(U + v * N, sl.g.nx * sizeof(double), sl.U + v * sl.g.vs, sl.g.px * sizeof(double),
+                                 sl.g.nx * sizeof(double), (size_t)sl.g.ny * sl.g.nz, cudaMemcpyDeviceToHost,
+                                 b->stream));
     SB_TRY(cudaStreamSynchronize(b->stream));
     return SETB_OK;
 }
@@ -487,6 +499,7 @@ int32_t setb_batch_status(setb_batch* b, int32_t slot, setb_diag* out) {
     out->n_wave_err = (int64_t)s.n_wave;
     out->n_recon_err = (int64_t)s.n_recon;
     out->n_fp64_redo = (int64_t)s.n_redo;
+    if (s.n_timeout) return SETB_ETIMEOUT;
     if (s.n_negdens) return SETB_ENEGDENS;
     if (s.n_wave) return SETB_EWAVES;
     if (s.n_recon) return SETB_ERECON;

@@ -31,6 +31,8 @@ struct setb_handle {
     DevStatus* st = nullptr;
     DevClock* h_clk = nullptr;             // pinned mirrors
     DevStatus* h_st = nullptr;
+    CUtensorMap* tmap = nullptr;           // device: [buffer 0/1][tile shape: plain/delta, mixed]
+    bool tma_ok[2] = {false, false};       // per tile shape: maps encoded (else plain loads)
     int ctas_per_sm = 1;
     int sm_count = 148;
 };
@@ -73,10 +75,7 @@ GridGeom make_geom(const setb_cart_desc* d) {
     g.nx = d->nx;
     g.ny = d->ny;
     g.nz = d->nz;
-    g.px = d->nx;
-    g.ps = (long long)d->nx * d->ny;
-    g.vs = g.ps * d->nz;
-    g.vs = (g.vs + 31) / 32 * 32;   // keep every variable plane 256-byte aligned
+    set_device_strides(g);   // even row pitch, 256-byte aligned variable planes
     const int n[3] = {d->nx, d->ny, d->nz};
     for (int a = 0; a < 3; a++) {
         g.lo[a] = d->lo[a];
@@ -149,6 +148,7 @@ int download_clock(setb_handle* h) {
 }
 
 int status_code(const DevStatus& s) {
+    if (s.n_timeout) return SETB_ETIMEOUT;
     if (s.n_negdens) return SETB_ENEGDENS;
     if (s.n_wave) return SETB_EWAVES;
     if (s.n_recon) return SETB_ERECON;
@@ -166,6 +166,7 @@ void destroy_impl(setb_handle* h) {
     if (h->comp) cudaFree(h->comp);
     if (h->clk) cudaFree(h->clk);
     if (h->st) cudaFree(h->st);
+    if (h->tmap) cudaFree(h->tmap);
     if (h->h_clk) cudaFreeHost(h->h_clk);
     if (h->h_st) cudaFreeHost(h->h_st);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -200,6 +201,27 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
     const size_t bytes = sizeof(double) * 8 * (size_t)h->g.vs;
     for (int b = 0; b < 2; b++) {
         if (cudaMalloc(&h->buf[b], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            destroy_impl(h);
+            return SETB_ENOMEM;
+        }
+        // row padding and the tail of every variable plane stay zero
+        if (cudaMemsetAsync(h->buf[b], 0, bytes, h->stream) != cudaSuccess) {
+            destroy_impl(h);
+            return SETB_ECUDA;
+        }
+    }
+    {
+        CUtensorMap tm[4] = {};
+        for (int shape = 0; shape < 2; shape++) {
+            h->tma_ok[shape] = true;
+            for (int b = 0; b < 2; b++)
+                if (encode_state_tmap(h->g, h->buf[b], shape == 0 ? 0 : 1, &tm[2 * b + shape]) != SETB_OK)
+                    h->tma_ok[shape] = false;
+        }
+        if (cudaMalloc(&h->tmap, sizeof(tm)) != cudaSuccess ||
+            cudaMemcpyAsync(h->tmap, tm, sizeof(tm), cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess) {
             cudaGetLastError();
             destroy_impl(h);
             return SETB_ENOMEM;
@@ -403,12 +425,16 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     a.st = h->st;
     a.cfl = o->cfl;
     a.n_disc = o->n_disc;
+    const int shape = P == 1 ? 1 : 0;
     if (ev) SB_TRY(cudaEventRecord(ev[0], h->stream));
     for (int s = 0; s < nsteps; s++) {
         double* U = h->buf[h->cur];
         double* W = h->buf[1 - h->cur];
+        const CUtensorMap* tmU = h->tma_ok[shape] ? h->tmap + 2 * h->cur + shape : nullptr;
+        const CUtensorMap* tmW = h->tma_ok[shape] ? h->tmap + 2 * (1 - h->cur) + shape : nullptr;
         if (o->scheme == 2) {
             a.Uin = U;
+            a.tm_in = tmU;
             a.Ubase = nullptr;
             a.Uout = W;
             a.finalize = 0;
@@ -416,6 +442,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
             SB_TRY(launch_stage(a, P, o->n_state, o->order, 0, true, h->stream));
             if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
             a.Uin = W;
+            a.tm_in = tmW;
             a.Ubase = U;
             a.Uout = U;
             a.finalize = 1;
@@ -424,6 +451,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
             if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
         } else {
             a.Uin = U;
+            a.tm_in = tmU;
             a.Ubase = nullptr;
             a.Uout = W;
             a.finalize = 1;
@@ -553,8 +581,9 @@ int32_t setb_get_conserved(setb_handle* h, double* U) {
     cudaSetDevice(h->device);
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
     for (int v = 0; v < 8; v++)
-        SB_TRY(cudaMemcpyAsync(U + v * N, h->buf[h->cur] + v * h->g.vs, N * sizeof(double), cudaMemcpyDeviceToHost,
-                               h->stream));
+        SB_TRY(cudaMemcpy2DAsync(U + v * N, h->g.nx * sizeof(double), h->buf[h->cur] + v * h->g.vs,
+                                 h->g.px * sizeof(double), h->g.nx * sizeof(double), (size_t)h->g.ny * h->g.nz,
+                                 cudaMemcpyDeviceToHost, h->stream));
     SB_TRY(cudaStreamSynchronize(h->stream));
     return SETB_OK;
 }

@@ -1,6 +1,7 @@
 // setb_internal.cuh -- device-side structures shared by the stage kernels and the host runtime.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "mhd_core.cuh"
 
@@ -35,12 +36,15 @@ struct DevClock {
 struct DevStatus {
     unsigned long long n_negdens, n_pfloor, n_wave, n_recon, n_redo;
     unsigned long long first_bad;   // ULLONG_MAX when none
+    unsigned long long n_timeout;   // bounded waits on a plane copy that gave up
 };
 
 // Geometry + boundary data of one Cartesian grid.
 struct GridGeom {
     int nx, ny, nz, lz;             // lz: z extent of one CTA's march
-    long long vs, ps, px;           // var / plane / row strides of the SoA state (elements)
+    long long vs, ps, px;           // var / plane / row strides of the SoA state (elements);
+                                    // device-owned states keep px even and vs a multiple of 32
+                                    // (16-byte rows for the tensor copies, 256-byte planes)
     double lo[3], h[3];
     double square[3];               // face areas: hy*hz, hx*hz, hx*hy
     double inv_vol;                 // 1/(hx*hy*hz)
@@ -63,6 +67,9 @@ struct StageArgs {
                                         // (Euler / Heun stage 2); null = plain update
     unsigned total_tiles;               // batch: tiles of this solve in the launch
     int n_state;                        // batch: per-solve Riemann solver (2 HLLC, 3 HLLD)
+    const CUtensorMap* tm_in;           // tensor map of Uin (device memory) for the plane
+                                        // copies, box (kTileX + 4, ty + 4, 1, 8) of this form's
+                                        // tile; null = planes read with plain loads
 };
 
 // One launch of the batch kernel: tiles of many solves behind one work-queue counter.
@@ -282,6 +289,18 @@ SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const d
     sp[2] = SM;
     *flag = fl;
 }
+
+// Row pitch and variable stride of a device-owned state of this geometry.
+inline void set_device_strides(GridGeom& g) {
+    g.px = (g.nx + 1) / 2 * 2;
+    g.ps = g.px * g.ny;
+    g.vs = (g.ps * g.nz + 31) / 32 * 32;
+}
+
+// Encodes the 4-D tensor map (x, y, z, variable) of the FP64 SoA state at `base` with geometry
+// g, box (kTileX + 4, tile_shape(precision).ty + 4, 1, 8): one plane of a column tile with its
+// 2-cell halo.  Returns a SETB_* status.
+int encode_state_tmap(const GridGeom& g, const double* base, int precision, CUtensorMap* out);
 
 // ---------------------------------------------------------------- launch entry points
 cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int kind, bool want_dt,

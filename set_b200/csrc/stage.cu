@@ -81,6 +81,77 @@ __device__ __forceinline__ void load_plane(const StageArgs& A, RT* dst, int i0, 
     }
 }
 
+// ---- plane copies by the tensor-memory accelerator
+// One copy per plane: the (kTileX + 4) x (TY + 4) x 1 x 8 box of the state at (i0-2, j0-2, k, 0)
+// lands in the staging buffer as [variable][y][x]; its completion is counted on an mbarrier.
+// Coordinates outside the grid read zeros (the boundary rules are applied when the plane is
+// converted); x = i0 - 2 is even, so the copy starts on a 16-byte boundary.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for phase `parity` of the barrier, for at most ~2 s of SM clock; false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > 4000000000ll) return false;
+    return true;
+}
+
+// Issued by one thread: expects `bytes` on the barrier and starts the copy.  The caller has
+// ordered earlier generic-proxy reads of `dst` before this (barrier + proxy fence).
+__device__ __forceinline__ void tma_plane(void* dst, const CUtensorMap* tm, int x, int y, int z, unsigned bytes,
+                                          unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(smem_u32(dst)),
+        "l"(tm), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Primitive plane with the boundary rules from a staged box (conserved, [v][y][x] with row HX):
+// inflow beyond x = hi, zero-gradient (clamped index, always inside the box) elsewhere.
+template <int P, typename RT>
+__device__ __forceinline__ void convert_plane(const StageArgs& A, const double* stg, RT* dst, int i0, int j0) {
+    constexpr int HX = Tile<P>::HX, PLANE = Tile<P>::PLANE, NT = Tile<P>::NT;
+    const GridGeom& g = A.g;
+    for (int c = threadIdx.x; c < PLANE; c += NT) {
+        const int cx = c % HX, cy = c / HX;
+        const int i = i0 - 2 + cx, j = j0 - 2 + cy;
+        double q[8];
+        if (i >= g.nx) {
+#pragma unroll
+            for (int v = 0; v < 8; v++) q[v] = g.inflow[v];
+        } else {
+            const int sx = max(i, 0) - (i0 - 2), sy = min(max(j, 0), g.ny - 1) - (j0 - 2);
+            const double* src = stg + sy * HX + sx;
+            double U[8];
+#pragma unroll
+            for (int v = 0; v < 8; v++) U[v] = src[v * PLANE];
+            double ke, me;
+            prim_from_cons(U, q, ke, me);
+        }
+#pragma unroll
+        for (int v = 0; v < 8; v++) dst[v * PLANE + c] = (RT)q[v];
+    }
+}
+
 // Face-frame order (normal, t1, t2) of the components of a face normal to axis AX: entry v of
 // the face-frame state is natural component face_perm<AX>(v) of (rho, u, v, w, p, Bx, By, Bz).
 template <int AX> __host__ __device__ constexpr int face_perm(int v) {
@@ -165,15 +236,18 @@ __device__ __noinline__ int face_fp64_states(const double* q1, const double* q2,
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
-__device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int bz, unsigned total_tiles) {
+__device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int bz, unsigned total_tiles,
+                                         unsigned long long* bar, unsigned& n_waits) {
     using RG = typename Types<P>::Ring;
     using FT = typename Types<P>::Flux;
     using RT = typename Types<P>::Math;
     using C = Tile<P>;
     constexpr int TX = C::TX, TY = C::TY, NC = C::NC, NT = C::NT, HX = C::HX, PLANE = C::PLANE;
     constexpr int NXF = C::NXF, NYF = C::NYF;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    RG* ring = reinterpret_cast<RG*>(smem_raw);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // [8][PLANE] staged conserved box; tensor copies land on a 128-byte aligned address
+    double* stg = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    RG* ring = reinterpret_cast<RG*>(stg + 8 * PLANE);
     FT* fx = reinterpret_cast<FT*>(ring + RING * 8 * PLANE);   // [8][NXF]
     FT* fy = fx + 8 * NXF;                                      // [8][NYF]
     __shared__ double red[NT / 32];
@@ -300,16 +374,35 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         if (WANT_DT && real) rate = fmax(rate, fmax(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
     };
 
-    // ---- the march.  Iteration k0-1 is the prologue: planes k0-2 .. k0+1 and only the z face
-    // k0-1/2 (carried into the first update).  Every face goes through the one do_face call
-    // site below, so a face's arithmetic does not depend on where a chunk starts.
-    for (int kk = k0 - 2; kk <= k0; kk++) load_plane<P, RG>(A, ring + ring_slot(kk) * 8 * PLANE, i0, j0, kk);
+    // ---- the march over planes kk = k0-2 .. k1+1.  Plane kk enters ring slot kk; from
+    // kk = k0+1 on, iteration k = kk-2 computes the faces of plane k and (from k = k0) updates
+    // it.  Iteration k0-1 is the prologue: only the z face k0-1/2 (carried into the first
+    // update).  Every face goes through the one do_face call site below, so a face's arithmetic
+    // does not depend on where a chunk starts.  With a tensor map, the copy of plane kk+1 is in
+    // flight while plane kk's faces and updates run; the last copy issued is plane k1+1.
+    const bool use_tma = A.tm_in != nullptr;
+    constexpr unsigned kPlaneBytes = 8u * PLANE * sizeof(double);
+    const int kz_last = k1 + 1;
+    auto issue_copy = [&](int kk) {
+        tma_plane(stg, A.tm_in, i0 - 2, j0 - 2, min(max(kk, 0), g.nz - 1), kPlaneBytes, bar);
+    };
+    if (use_tma && t == 0) issue_copy(k0 - 2);
     double fzl[8];
     const int gi = i0 + tx, gj = j0 + ty;
     const bool own = (t < NC) && (gi < g.nx) && (gj < g.ny);
-    for (int k = k0 - 1; k < k1; k++) {
-        load_plane<P, RG>(A, ring + ring_slot(k + 2) * 8 * PLANE, i0, j0, k + 2);
+    for (int kk = k0 - 2; kk <= kz_last; kk++) {
+        RG* slot = ring + ring_slot(kk) * 8 * PLANE;
+        if (use_tma) {
+            if (!mbar_wait_bounded(bar, n_waits & 1u)) atomicAdd(&A.st->n_timeout, 1ull);
+            n_waits++;
+            convert_plane<P, RG>(A, stg, slot, i0, j0);
+        } else {
+            load_plane<P, RG>(A, slot, i0, j0, kk);
+        }
         __syncthreads();
+        if (use_tma && t == 0 && kk < kz_last) issue_copy(kk + 1);
+        const int k = kk - 2;
+        if (k < k0 - 1) continue;
         const bool pro = (k < k0);
         const int njobs = pro ? JZ : JOBS;
         for (int job = warp; job < njobs; job += NW) do_face(job, k, pro && k0 > 0);
@@ -437,8 +530,12 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
 __global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) stage_kernel(const StageArgs A) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) mbar_init(&bar);
+    __syncthreads();
+    unsigned n_waits = 0;
     run_tile<P, NSTATE, ORDER, KIND, WANT_DT>(A, blockIdx.x, blockIdx.y, blockIdx.z,
-                                               gridDim.x * gridDim.y * gridDim.z);
+                                               gridDim.x * gridDim.y * gridDim.z, &bar, n_waits);
 }
 
 // Persistent batch kernel: each CTA takes tiles from the work queue until it is empty; the
@@ -448,8 +545,11 @@ template <int P, int ORDER, int KIND, bool WANT_DT>
 __global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) batch_stage_kernel(const BatchArgs B) {
     __shared__ __align__(16) StageArgs As;
     __shared__ int4 it;
+    __shared__ __align__(8) unsigned long long bar;
     constexpr int WORDS = sizeof(StageArgs) / sizeof(unsigned long long);
     static_assert(sizeof(StageArgs) % sizeof(unsigned long long) == 0, "StageArgs must be 8-byte granular");
+    if (threadIdx.x == 0) mbar_init(&bar);
+    unsigned n_waits = 0;   // completed phases of `bar`, the same count in every thread
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned i = atomicAdd(B.queue, 1u);
@@ -463,15 +563,16 @@ __global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) batch_stage_kernel
         for (int q = threadIdx.x; q < WORDS; q += Tile<P>::NT) dst[q] = src[q];
         __syncthreads();
         if (As.n_state == 3)
-            run_tile<P, 3, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles);
+            run_tile<P, 3, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
         else
-            run_tile<P, 2, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles);
+            run_tile<P, 2, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
     }
 }
 
+// Dynamic shared memory: alignment slack, staged box (FP64), primitive ring, x / y flux buffers.
 template <int P>
 constexpr int smem_bytes() {
-    return RING * 8 * Tile<P>::PLANE * (int)sizeof(typename Types<P>::Ring) +
+    return 128 + 8 * Tile<P>::PLANE * (int)sizeof(double) + RING * 8 * Tile<P>::PLANE * (int)sizeof(typename Types<P>::Ring) +
            8 * (Tile<P>::NXF + Tile<P>::NYF) * (int)sizeof(typename Types<P>::Flux);
 }
 
