@@ -45,13 +45,14 @@ enum : int { kFlagWave = 1, kFlagStar = 2 };
 
 // ------------------------------------------------------------------ elementary functions
 // FP64: IEEE square root and correctly rounded reciprocal.  FP32 (the mixed form's Riemann
-// arithmetic): the hardware approximations (MUFU rsqrt / reciprocal, ~2 ulp).
+// arithmetic): the special-function unit's approximations (PTX sqrt / rcp / rsqrt .approx.ftz,
+// a few ulp, subnormals flushed -- states here are far from the FP32 subnormal range).
 SB_HD double sb_sqrt(double x) { return sqrt(x); }
 SB_HD float sb_sqrt(float x) {
-#if defined(__CUDA_ARCH__) && defined(SB_FP32_IEEE)
-    return __fsqrt_rn(x);
-#elif defined(__CUDA_ARCH__)
-    return x > 0.0f ? x * rsqrtf(x) : 0.0f;
+#if defined(__CUDA_ARCH__)
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 #else
     return std::sqrt(x);
 #endif
@@ -64,10 +65,10 @@ SB_HD double sb_rcp(double x) {
 #endif
 }
 SB_HD float sb_rcp(float x) {
-#if defined(__CUDA_ARCH__) && defined(SB_FP32_IEEE)
-    return __frcp_rn(x);
-#elif defined(__CUDA_ARCH__)
-    return __fdividef(1.0f, x);
+#if defined(__CUDA_ARCH__)
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 #else
     return 1.0f / x;
 #endif
@@ -81,7 +82,9 @@ SB_HD double sb_rsqrt(double x) {
 }
 SB_HD float sb_rsqrt(float x) {
 #if defined(__CUDA_ARCH__)
-    return rsqrtf(x);
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
 #else
     return 1.0f / std::sqrt(x);
 #endif
@@ -91,8 +94,13 @@ template <typename T> SB_HD T sb_min(T a, T b) { return b < a ? b : a; }
 template <typename T> SB_HD T sb_max(T a, T b) { return a < b ? b : a; }
 template <typename T> SB_HD T sb_pos(T x) { return x > T(0) ? x : T(0); }
 
-// Solvers.f90:126-137: (signum(x)+signum(y))/2 * min(|x|,|y|)
+// Solvers.f90:126-137: (signum(x)+signum(y))/2 * min(|x|,|y|).  FP32 on the device is
+// branch-free: |minmod| = max(0, min(|a|, b * sign(a))) with the sign of a (the same value for
+// every finite a, b, except that a zero result may carry a's sign).
 template <typename T> SB_HD T minmod(T a, T b) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 4) return copysignf(fmaxf(0.0f, fminf(fabsf(a), b * copysignf(1.0f, a))), a);
+#endif
     if (a > T(0) && b > T(0)) return sb_min(a, b);
     if (a < T(0) && b < T(0)) return sb_max(a, b);
     return T(0);
