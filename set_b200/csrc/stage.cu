@@ -25,6 +25,7 @@
 // P = 2, delta form: FP64 ring and fluxes, the Riemann solver's small differences in FP32.
 #include <cfloat>
 #include <type_traits>
+#include "riemann_f32x2.cuh"
 #include "setb_internal.cuh"
 
 namespace sb {
@@ -350,7 +351,14 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             }
         } else {
             RT SL, SR, SM;
-            fl = riemann<RT, NSTATE, false, P == 1>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+            if constexpr (P == 1 && NSTATE >= 2) {
+                if (A.n_disc == 0)
+                    fl = riemann_f32x2<NSTATE>(q1, q2, F, SL, SR, SM);
+                else
+                    fl = riemann<RT, NSTATE, false, true>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+            } else {
+                fl = riemann<RT, NSTATE, false, P == 1>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+            }
             sl = (double)SL;
             sr = (double)SR;
         }
