@@ -37,6 +37,10 @@ sys.path.insert(0, ROOT)
 BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
 BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
 BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
+# DRAM bytes (read + write) per cell of one plain stage-2 launch, from the ncu capture at 160^3
+# summarised in profiles/stage_plain_hlld_160cube.md (775.97 MB / 4.096 M cells); traffic grows
+# with the cell count, so the full-size launch's traffic is this figure times its cells.
+TRAFFIC_STAGE2_PER_CELL = 775.966208e6 / 160 ** 3
 
 
 def peaks():
@@ -348,6 +352,7 @@ def run_ours(args, world, rank, local):
                   "latency_p50_s": out["latency_p50_s"], "latency_p99_s": out["latency_p99_s"],
                   "solves_per_s": out["solves_per_s"], "span_s": out["span_s"], "max_active": out["max_active"],
                   "converged": out["converged"], "failed": out["failed"],
+                  "failed_by_status": out["failed_by_status"],
                   "sequential_plain_solves_per_s": seq["solves_per_s"],
                   "speedup_vs_sequential_plain": out["solves_per_s"] / seq["solves_per_s"]}
 
@@ -366,9 +371,11 @@ def run_ours(args, world, rank, local):
             "config": config_dict(args),
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": cells * 64,
                     "d2h_bytes_per_step": cells * 64},
-            "roofline": {"bound": "hbm", "kernel": "stage_fp64_kernel<HLLD,minmod,stage2>",
+            "roofline": {"bound": "hbm", "kernel": "stage_kernel<plain FP64, HLLD, minmod, Heun stage 2>",
                          "achieved": ach2, "peak": hbm, "unit": "GB/s", "frac": ach2 / hbm,
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind, "traffic": TRAFFIC_STAGE2_PER_CELL * cells,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 160^3, "
+                                           "scaled by cells",
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
                          "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2}},
             "mixed": mixed,

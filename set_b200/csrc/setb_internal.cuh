@@ -146,13 +146,8 @@ SB_HD void prim_from_cons_exact(const double* U, double* q) {
 }
 
 // Source state (primitive) at cell (i,j,k); false when the cell is outside r_src.
-SB_HD bool source_prim(const GridGeom& g, int i, int j, int k, double* q) {
-    if (!(g.r_src > 0.0)) return false;
-    const double x = cell_coord(g.lo[0], i, g.h[0]);
-    const double y = cell_coord(g.lo[1], j, g.h[1]);
-    const double z = cell_coord(g.lo[2], k, g.h[2]);
-    const double r2 = dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
-    if (!(r2 < dmul(g.r_src, g.r_src))) return false;
+// Source state at centre (x, y, z) with r2 = (x^2 + y^2) + z^2 already below r_src^2.
+SB_HD void source_state(const GridGeom& g, double x, double y, double z, double r2, double* q) {
     const double r = sqrt(r2);
     const double re = r > g.r_floor ? r : g.r_floor;
     const double s = g.r_src / re;
@@ -167,6 +162,16 @@ SB_HD bool source_prim(const GridGeom& g, int i, int j, int k, double* q) {
     }
     q[4] = dmul(g.p_over_rho_src, rho);
     q[5] = q[6] = q[7] = 0.0;
+}
+
+SB_HD bool source_prim(const GridGeom& g, int i, int j, int k, double* q) {
+    if (!(g.r_src > 0.0)) return false;
+    const double x = cell_coord(g.lo[0], i, g.h[0]);
+    const double y = cell_coord(g.lo[1], j, g.h[1]);
+    const double z = cell_coord(g.lo[2], k, g.h[2]);
+    const double r2 = dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
+    if (!(r2 < dmul(g.r_src, g.r_src))) return false;
+    source_state(g, x, y, z, r2, q);
     return true;
 }
 

@@ -395,7 +395,12 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         tma_plane(stg, A.tm_in, i0 - 2, j0 - 2, min(max(kk, 0), g.nz - 1), kPlaneBytes, bar);
     };
     if (use_tma && t == 0) issue_copy(k0 - 2);
-    double fzl[8];
+    double fzl[8];   // z fluxes k-1/2 (carried) and k+1/2 of this thread's column
+    // centre of this thread's column and its part of the source-sphere test
+    const double cxs = cell_coord(g.lo[0], i0 + tx, g.h[0]), cys = cell_coord(g.lo[1], j0 + ty, g.h[1]);
+    const double xy2 = dadd(dmul(cxs, cxs), dmul(cys, cys));
+    const double rsrc2 = dmul(g.r_src, g.r_src);
+    const bool col_src = g.r_src > 0.0 && xy2 < rsrc2;
     const int gi = i0 + tx, gj = j0 + ty;
     const bool own = (t < NC) && (gi < g.nx) && (gj < g.ny);
     for (int kk = k0 - 2; kk <= kz_last; kk++) {
@@ -430,7 +435,16 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             const long long off = (long long)k * g.ps + (long long)gj * g.px + gi;
             double un[8], qs[8];
             bool reset_comp = false;
-            if (source_prim(g, gi, gj, k, qs)) {
+            bool is_src = false;
+            if (col_src) {   // (x^2 + y^2) + z^2 < r_src^2, rounded as in source_prim
+                const double cz = cell_coord(g.lo[2], k, g.h[2]);
+                const double r2 = dadd(xy2, dmul(cz, cz));
+                if (r2 < rsrc2) {
+                    source_state(g, cxs, cys, cz, r2, qs);
+                    is_src = true;
+                }
+            }
+            if (is_src) {
                 cons_from_prim_exact(qs, un);
                 reset_comp = true;
             } else {

@@ -87,9 +87,14 @@ def run_stream(requests, max_slots: int = 256, precision: int = 1, hbm_budget: i
         stats = srv.stats()
     lat = np.array([r.t_done - r.t_submit for r in results])
     span = max(r.t_done for r in results) - min(r.t_submit for r in results)
+    failed_by_status = {}
+    for r in results:
+        if r.status != 0:
+            name = lib().setb_strerror(int(r.status)).decode()
+            failed_by_status[name] = failed_by_status.get(name, 0) + 1
     return {"latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
             "solves_per_s": len(results) / span, "span_s": span, "results": results, "states": states,
-            "max_active": stats["max_active"], "failed": stats["failed"],
+            "max_active": stats["max_active"], "failed": stats["failed"], "failed_by_status": failed_by_status,
             "steps": [r.steps for r in results], "converged": int(sum(r.converged for r in results))}
 
 
