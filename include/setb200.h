@@ -181,6 +181,45 @@ SETB_API int32_t setb_stream(setb_handle* h, void** stream);
 
 SETB_API int32_t setb_destroy(setb_handle* h);
 
+/* ------------------------------------------------------------------ face-list grids
+ * The reference's own geometry: an explicit list of cells and faces, as Set_CUDA uploads it
+ * (cuf_kernel.cuf:351-382) from the STORAGE arrays (Storage_module.f90:20-37), in their Fortran
+ * layouts and 1-based numbering:
+ *   cell_par     Cell_par(16,N)         primitive state, columns 1..8 used
+ *   cell_center  Cell_center(3,N)       cell_volume  Cell_Volume(N)
+ *   cell_gran    Cell_gran(6,N)         face numbers of each cell, 0 = none
+ *   gran_normal  Gran_normal(3,G)       unit normal, pointing from neighbour 1 to neighbour 2
+ *   gran_square  Gran_square(G)         face area
+ *   gran_center  Gran_center(3,G)
+ *   gran_neighbour      Gran_neighbour(2,G)      cells on each side; neighbour 2 = -1 on a wall
+ *   gran_neighbour_tvd  Gran_neighbour_TVD(2,G)  far cells of the TVD stencil, -1 = none
+ *   gran_type    Gran_type(G)           1 other, 2 ordinary (a wall when neighbour 2 is -1),
+ *                                       3 inner sphere, 4 outer boundary (ghost = cell with its
+ *                                       normal velocity clamped to <= -0.1), 5 axis (ghost =
+ *                                       cell with v mirrored)  (cuf_solvers.cuf:318-345)
+ * The flux of a face is computed once per stage and added to neighbour 1 and subtracted from
+ * neighbour 2 (cuf_solvers.cuf:691-703).  A handle made here is driven by setb_step,
+ * setb_step_profiled, setb_get_state, setb_set_state, setb_get_conserved, setb_status and
+ * setb_destroy like a Cartesian one; it supports precision 0 (plain FP64).  Indices are checked
+ * on the host: an index outside its array, a non-positive volume or an unknown face type gives
+ * SETB_EINVAL. */
+typedef struct {
+    double r_src, rho_src, v_src, p_over_rho_src, r_floor;   /* source sphere, r_src 0 = none  */
+    double dt_init;             /* dt of the first step (reference: 2e-9, cuf_kernel.cuf:758)    */
+    double face_skip_radius;    /* faces whose neighbour-1 centre is nearer the origin than this
+                                   keep their previous flux (reference: 0.02, cuf_solvers.cuf:284);
+                                   0 = none                                                      */
+    double cell_freeze_radius;  /* cells nearer the origin are not updated (reference: 0.05,
+                                   cuf_solvers.cuf:611); 0 = none                                */
+} setb_fl_params;
+
+/* Replaces Set_CUDA for the reference's grid (cuf_kernel.cuf:351-382). */
+SETB_API int32_t setb_init_facelist(setb_handle** h, int32_t n_cell, int32_t n_gran, const double* cell_par,
+                                    const double* cell_center, const double* cell_volume, const int32_t* cell_gran,
+                                    const double* gran_normal, const double* gran_square, const double* gran_center,
+                                    const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd,
+                                    const int32_t* gran_type, const setb_fl_params* params);
+
 /* ------------------------------------------------------------------ batched solves
  * No counterpart in the reference (one grid per process, cuf_kernel.cuf:351-382).  A batch
  * advances many Cartesian solves of uneven size together: every step is two persistent launches

@@ -232,3 +232,47 @@ def cellpar_to_cons(cp: np.ndarray, shape) -> np.ndarray:
 
 def max_threads() -> int:
     return lib().orc_max_threads()
+
+
+# ---------------------------------------------------------------------------- face-list grids
+class OrcFaceList(C.Structure):
+    _fields_ = [("n_cell", C.c_int64), ("n_gran", C.c_int64),
+                ("cell_center", _dp), ("cell_volume", _dp), ("cell_gran", C.POINTER(C.c_int32)),
+                ("gran_normal", _dp), ("gran_square", _dp), ("gran_center", _dp),
+                ("gran_neighbour", C.POINTER(C.c_int32)), ("gran_neighbour_tvd", C.POINTER(C.c_int32)),
+                ("gran_type", C.POINTER(C.c_int32)),
+                ("r_src", C.c_double), ("rho_src", C.c_double), ("v_src", C.c_double),
+                ("p_over_rho_src", C.c_double), ("r_floor", C.c_double), ("dt_init", C.c_double),
+                ("face_skip_radius", C.c_double), ("cell_freeze_radius", C.c_double)]
+
+
+def facelist(mesh, params) -> OrcFaceList:
+    """Oracle view of a face list (arrays in the reference's layouts, 1-based) and its
+    parameters (anything with the fields of setb_fl_params).  Keep `mesh` alive while used."""
+    m = OrcFaceList()
+    m.n_cell, m.n_gran = mesh.n_cell, mesh.n_gran
+    i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+    m.cell_center, m.cell_volume, m.cell_gran = _p(mesh.cell_center), _p(mesh.cell_volume), i32(mesh.cell_gran)
+    m.gran_normal, m.gran_square, m.gran_center = _p(mesh.gran_normal), _p(mesh.gran_square), _p(mesh.gran_center)
+    m.gran_neighbour, m.gran_neighbour_tvd, m.gran_type = (i32(mesh.gran_neighbour), i32(mesh.gran_neighbour_tvd),
+                                                          i32(mesh.gran_type))
+    for f in ("r_src", "rho_src", "v_src", "p_over_rho_src", "r_floor", "dt_init", "face_skip_radius",
+              "cell_freeze_radius"):
+        setattr(m, f, float(getattr(params, f)))
+    return m
+
+
+def fl_run(m: OrcFaceList, o: OrcOpts, U: np.ndarray, nsteps: int, clock: OrcClock | None = None,
+           flux: np.ndarray | None = None, nthreads=0):
+    """Advance the face-list state U[8, N] (conserved, modified in place) by nsteps with the
+    persistent face flux array `flux` [G, 9] (zeros when None).  Returns (clock, diag, flux)."""
+    if clock is None:
+        clock = OrcClock()
+        clock.time_all, clock.dt_next, clock.dt_last = 0.0, m.dt_init, 0.0
+    if flux is None:
+        flux = np.zeros((m.n_gran, 9))
+    dg = OrcDiag()
+    dg.first_bad_cell = -1
+    lib().orc_fl_run(C.byref(m), C.byref(o), _p(U), _p(flux), C.byref(clock), int(nsteps), int(nthreads),
+                     C.byref(dg))
+    return clock, dg, flux

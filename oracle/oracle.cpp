@@ -16,7 +16,8 @@
 //   * time loop (lagged dt: a step uses the dt reduced in the previous step's first stage;
 //     first dt = 2e-9; reset value 1e15) ...................... SET_Fortran_Cuda_MHD/cuf_kernel.cuf:758, 780-925
 // on a uniform Cartesian grid whose face lists are implicit (the reference's face-list
-// geometry with dist = h/2, df = h/2, dff = 3h/2, square = h_b*h_c, volume = hx*hy*hz).
+// geometry with dist = h/2, df = h/2, dff = 3h/2, square = h_b*h_c, volume = hx*hy*hz), and on
+// an explicit face list (orc_fl_run: cells, faces, face types 2/4/5, TVD neighbours).
 //
 // Parity pinning.  The reference ships no tests, fixtures or golden vectors, and its Fortran
 // path cannot be compiled here (no Fortran compiler).  The n_state <= 1 (HLL) branch of chlld,
@@ -884,5 +885,221 @@ void orc_stage(const orc_grid* g, const orc_opts* o, const double* Uin, const do
 }
 
 int orc_max_threads(void) { return omp_get_max_threads(); }
+
+// ============================================================================ face-list grid
+// The reference's own geometry (Storage_module.f90:20-37): explicit cells and faces with the
+// Fortran layouts Cell_center(3,N), Cell_Volume(N), Cell_gran(6,N) (1-based face numbers, 0 =
+// none), Gran_normal(3,G), Gran_square(G), Gran_center(3,G), Gran_neighbour(2,G) and
+// Gran_neighbour_TVD(2,G) (1-based cell numbers, -1 = none), Gran_type(G).  The face flux
+// array Gran_POTOK(9,G) persists between stages (a skipped face keeps its previous flux).
+typedef struct {
+    int64_t n_cell, n_gran;
+    const double* cell_center;
+    const double* cell_volume;
+    const int32_t* cell_gran;
+    const double* gran_normal;
+    const double* gran_square;
+    const double* gran_center;
+    const int32_t* gran_neighbour;
+    const int32_t* gran_neighbour_tvd;
+    const int32_t* gran_type;
+    double r_src, rho_src, v_src, p_over_rho_src, r_floor;   // source sphere (r_src 0 = none)
+    double dt_init;
+    double face_skip_radius;    // faces whose first cell has |centre| < this are skipped
+    double cell_freeze_radius;  // cells with |centre| < this are not updated
+} orc_facelist;
+
+static double norm3(const double* x) { return std::sqrt((x[0] * x[0] + x[1] * x[1]) + x[2] * x[2]); }
+
+// One face, cuf_solvers.cuf:243-440: boundary ghost by face type, TVD through the far
+// neighbours with distance-weighted `linear`, chlld with the face normal, flux * area.
+// Returns the dt candidate (dt_face_cap when the face is skipped: it leaves F untouched).
+static double fl_face(const orc_facelist* m, const orc_opts* o, const double* P, int64_t gr, double* F,
+                      int64_t& nrec, int64_t& nwave) {
+    const int64_t s1 = m->gran_neighbour[2 * gr] - 1;
+    const int32_t s2r = m->gran_neighbour[2 * gr + 1];
+    const int type = m->gran_type[gr];
+    const double* c1 = m->cell_center + 3 * s1;
+    if (m->face_skip_radius > 0.0 && norm3(c1) < m->face_skip_radius) return dt_face_cap;   // :284
+    const double* gc = m->gran_center + 3 * gr;
+    const double* n = m->gran_normal + 3 * gr;
+    double rast[3];
+    for (int a = 0; a < 3; a++) rast[a] = gc[a] - c1[a];
+    const double dist = norm3(rast);
+    double q1[8], q2[8];
+    for (int v = 0; v < 8; v++) q1[v] = P[8 * s1 + v];
+    bool tvd = (o->order == 2);
+    const double* c2 = c1;
+    if (type == 4) {                              // :318-324 outer boundary
+        for (int v = 0; v < 8; v++) q2[v] = q1[v];
+        if (q2[1] > -0.1) q2[1] = -0.1;
+        tvd = false;
+    } else if (type == 5) {                       // :325-329 axis
+        for (int v = 0; v < 8; v++) q2[v] = q1[v];
+        q2[2] = -q2[2];
+        tvd = false;
+    } else if (type == 2 && s2r == -1) {          // :330-345 reflecting wall
+        const double vel = (n[0] * q1[1] + n[1] * q1[2]) + n[2] * q1[3];
+        for (int v = 0; v < 8; v++) q2[v] = q1[v];
+        for (int a = 0; a < 3; a++) {
+            const double vel1 = q1[1 + a] - vel * n[a];
+            const double vel2 = vel * n[a];
+            q2[1 + a] = vel1 - vel2;
+        }
+        tvd = false;
+    } else {
+        const int64_t s2 = s2r - 1;
+        for (int v = 0; v < 8; v++) q2[v] = P[8 * s2 + v];
+        c2 = m->cell_center + 3 * s2;
+    }
+    const int32_t ss1 = m->gran_neighbour_tvd[2 * gr], ss2 = m->gran_neighbour_tvd[2 * gr + 1];
+    if (tvd && ss1 >= 1 && ss2 >= 1) {           // :358-412
+        const double* cs1 = m->cell_center + 3 * (int64_t)(ss1 - 1);
+        const double* cs2 = m->cell_center + 3 * (int64_t)(ss2 - 1);
+        double r[3];
+        for (int a = 0; a < 3; a++) r[a] = gc[a] - c1[a];
+        const double df1 = norm3(r);
+        for (int a = 0; a < 3; a++) r[a] = gc[a] - c2[a];
+        const double df2 = norm3(r);
+        for (int a = 0; a < 3; a++) r[a] = gc[a] - cs1[a];
+        const double dff1 = norm3(r);
+        for (int a = 0; a < 3; a++) r[a] = gc[a] - cs2[a];
+        const double dff2 = norm3(r);
+        const double* q11 = P + 8 * (int64_t)(ss1 - 1);
+        const double* q22 = P + 8 * (int64_t)(ss2 - 1);
+        double t1[5], t2[5];
+        for (int v = 0; v < 5; v++) {
+            t1[v] = linear(-dff1, q11[v], -df1, q1[v], df2, q2[v], 0.0);
+            t2[v] = linear(-dff2, q22[v], -df2, q2[v], df1, q1[v], 0.0);
+        }
+        if (t1[0] < 0.0) t1[0] = q1[0];
+        if (t1[4] < 0.0) t1[4] = q1[4];
+        if (t2[0] < 0.0) t2[0] = q2[0];
+        if (t2[4] < 0.0) t2[4] = q2[4];
+        for (int v = 0; v < 5; v++) {
+            q1[v] = t1[v];
+            q2[v] = t2[v];
+        }
+    }
+    if (q1[0] < 0.0 || q2[0] < 0.0) nrec++;      // :414-420
+    double dsl, dsp, dsc, pot[8];
+    const double wc = 0.0;
+    const int rc = chlld(o->n_state, n[0], n[1], n[2], wc, q1, q2, dsl, dsp, dsc, pot, o->n_disc);
+    if (rc) {
+        nwave++;
+        for (int v = 0; v < 8; v++) pot[v] = 0.0;
+    }
+    const double sq = m->gran_square[gr];
+    for (int v = 0; v < 8; v++) F[v] = pot[v] * sq;   // :431
+    F[8] = 0.0;                                        // :433
+    return std::min(dt_face_cap, o->cfl * dist / (std::max(std::fabs(dsl), std::fabs(dsp)) + std::fabs(wc)));
+}
+
+// One stage on a face list (kind 0: Euler / Heun stage 1; kind 1: Heun stage 2).  U: conserved
+// SoA U[v*N + c]; F: the persistent Gran_POTOK(9,G).
+static void fl_stage(const orc_facelist* m, const orc_opts* o, const double* Uin, const double* Ubase,
+                     double* Uout, double* Fl, double dt, int kind, double* dt_min, orc_diag* dg, int nthreads) {
+    const int64_t N = m->n_cell, G = m->n_gran;
+    std::vector<double> P((size_t)N * 8);
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (int64_t c = 0; c < N; c++) {
+        double u8[8];
+        for (int v = 0; v < 8; v++) u8[v] = Uin[v * N + c];
+        prim_from_cons(u8, &P[(size_t)c * 8]);
+    }
+    double dmin = dt_reset;
+    int64_t nrec = 0, nwave = 0, nneg = 0, nfloor = 0, firstbad = -1;
+#pragma omp parallel for schedule(static) num_threads(nthreads) reduction(min : dmin) reduction(+ : nrec, nwave)
+    for (int64_t gr = 0; gr < G; gr++) dmin = std::min(dmin, fl_face(m, o, P.data(), gr, Fl + 9 * gr, nrec, nwave));
+    orc_grid sg{};   // the source sphere, through the Cartesian helper
+    sg.r_src = m->r_src;
+    sg.rho_src = m->rho_src;
+    sg.v_src = m->v_src;
+    sg.p_over_rho_src = m->p_over_rho_src;
+    sg.r_floor = m->r_floor;
+#pragma omp parallel num_threads(nthreads) reduction(+ : nneg, nfloor)
+    {
+        int64_t local_first = -1;
+#pragma omp for schedule(static)
+        for (int64_t c = 0; c < N; c++) {
+            const double* x = m->cell_center + 3 * c;
+            double un[8], qs[8];
+            if (m->cell_freeze_radius > 0.0 && norm3(x) < m->cell_freeze_radius) {   // :611
+                for (int v = 0; v < 8; v++) un[v] = kind == 0 ? Uin[v * N + c] : Ubase[v * N + c];
+            } else if (source_prim(&sg, x, qs)) {
+                cons_from_prim(qs, un);
+            } else {
+                double pot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int f = 0; f < 6; f++) {                                         // :691-703
+                    const int32_t j = m->cell_gran[6 * c + f];
+                    if (j == 0) continue;
+                    const double* Fj = Fl + 9 * (int64_t)(j - 1);
+                    const bool owner = m->gran_neighbour[2 * (int64_t)(j - 1)] == (int32_t)(c + 1);
+                    for (int v = 0; v < 8; v++) pot[v] = owner ? pot[v] + Fj[v] : pot[v] - Fj[v];
+                }
+                const double vol = m->cell_volume[c];
+                for (int v = 0; v < 8; v++) {
+                    if (kind == 0)
+                        un[v] = Uin[v * N + c] - dt * (pot[v] / vol);
+                    else
+                        un[v] = 0.5 * ((Ubase[v * N + c] + Uin[v * N + c]) - dt * (pot[v] / vol));
+                }
+                if (un[0] <= 0.0) {
+                    nneg++;
+                    if (local_first < 0) local_first = c;
+                    for (int v = 0; v < 8; v++) un[v] = Uin[v * N + c];
+                } else {
+                    double q[8];
+                    prim_from_cons(un, q);
+                    if (q[4] <= 0.0) {
+                        nfloor++;
+                        q[4] = p_floor;
+                        double u2[8];
+                        cons_from_prim(q, u2);
+                        un[4] = u2[4];
+                    }
+                }
+            }
+            for (int v = 0; v < 8; v++) Uout[v * N + c] = un[v];
+        }
+        if (local_first >= 0) {
+#pragma omp critical
+            {
+                if (firstbad < 0 || local_first < firstbad) firstbad = local_first;
+            }
+        }
+    }
+    *dt_min = std::min(*dt_min, dmin);
+    dg->n_recon_err += nrec;
+    dg->n_wave_err += nwave;
+    dg->n_negdens += nneg;
+    dg->n_pfloor += nfloor;
+    if (firstbad >= 0 && dg->first_bad_cell < 0) dg->first_bad_cell = firstbad;
+}
+
+// nsteps on a face list with the reference's loop semantics (lagged dt); F: Gran_POTOK(9,G),
+// persistent across calls.
+int orc_fl_run(const orc_facelist* m, const orc_opts* o, double* U, double* F, orc_clock* ck, int nsteps,
+               int nthreads, orc_diag* dg) {
+    const int64_t N = m->n_cell;
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+    std::vector<double> W((size_t)N * 8);
+    for (int s = 0; s < nsteps; s++) {
+        const double dt = ck->dt_next;
+        double dmin = dt_reset;
+        ck->time_all = ck->time_all + dt;
+        ck->dt_last = dt;
+        if (o->scheme == 1) {
+            fl_stage(m, o, U, nullptr, W.data(), F, dt, 0, &dmin, dg, nthreads);
+            std::memcpy(U, W.data(), sizeof(double) * N * 8);
+        } else {
+            fl_stage(m, o, U, nullptr, W.data(), F, dt, 0, &dmin, dg, nthreads);
+            double dummy = dt_reset;
+            fl_stage(m, o, W.data(), U, U, F, dt, 1, &dummy, dg, nthreads);
+        }
+        ck->dt_next = dmin;
+    }
+    return nsteps;
+}
 
 }  // extern "C"

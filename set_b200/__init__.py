@@ -103,6 +103,8 @@ _SIGS = {
     "setb_destroy": (C.c_int32, [C.c_void_p]),
     "setb_step_noalloc": (C.c_int32, [C.POINTER(CartDesc), C.POINTER(StepOpts), C.c_void_p, C.c_int64, C.c_int32,
                                       _dp, _dp, C.POINTER(Diag), C.c_void_p]),
+    "setb_init_facelist": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, _dp, _dp, _dp, _ip, _dp, _dp,
+                                       _dp, _ip, _ip, _ip, C.c_void_p]),
     "setb_batch_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int64]),
     "setb_batch_add": (C.c_int32, [C.c_void_p, C.POINTER(CartDesc), C.POINTER(LismIC), C.POINTER(StepOpts), _ip]),
     "setb_batch_remove": (C.c_int32, [C.c_void_p, C.c_int32]),

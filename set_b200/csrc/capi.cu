@@ -33,6 +33,7 @@ struct setb_handle {
     DevStatus* h_st = nullptr;
     CUtensorMap* tmap = nullptr;           // device: [buffer 0/1][tile shape: plain/delta, mixed]
     bool tma_ok[2] = {false, false};       // per tile shape: maps encoded (else plain loads)
+    FaceListDev* fl = nullptr;             // face-list grid (g is then 1-D: nx = N cells)
     int ctas_per_sm = 1;
     int sm_count = 148;
 };
@@ -167,6 +168,7 @@ void destroy_impl(setb_handle* h) {
     if (h->clk) cudaFree(h->clk);
     if (h->st) cudaFree(h->st);
     if (h->tmap) cudaFree(h->tmap);
+    if (h->fl) fl_destroy(h->fl);
     if (h->h_clk) cudaFreeHost(h->h_clk);
     if (h->h_st) cudaFreeHost(h->h_st);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -377,6 +379,49 @@ int32_t setb_init_cartesian(setb_handle** out, const setb_cart_desc* d, const do
     return rc;
 }
 
+int32_t setb_init_facelist(setb_handle** out, int32_t n_cell, int32_t n_gran, const double* cell_par,
+                           const double* cell_center, const double* cell_volume, const int32_t* cell_gran,
+                           const double* gran_normal, const double* gran_square, const double* gran_center,
+                           const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd, const int32_t* gran_type,
+                           const setb_fl_params* params) {
+    if (!out || !cell_par || !params || n_cell < 1 || n_gran < 1) return SETB_EINVAL;
+    *out = nullptr;
+    if (!(params->dt_init > 0.0)) return SETB_EINVAL;
+    int rc = fl_validate(n_cell, n_gran, cell_center, cell_volume, cell_gran, gran_normal, gran_square, gran_center,
+                         gran_neighbour, gran_neighbour_tvd, gran_type);
+    if (rc) return rc;
+    // the state lives in the handle's buffers as a 1-D "grid" of n_cell cells
+    setb_cart_desc d{};
+    d.nx = n_cell;
+    d.ny = d.nz = 1;
+    d.inflow[0] = d.inflow[4] = 1.0;   // unused by face lists (boundaries come from face types)
+    for (int a = 0; a < 3; a++) {
+        d.lo[a] = 0.0;
+        d.hi[a] = 1.0;
+    }
+    d.r_src = params->r_src;
+    d.rho_src = params->rho_src;
+    d.v_src = params->v_src;
+    d.p_over_rho_src = params->p_over_rho_src;
+    d.r_floor = params->r_floor;
+    d.dt_init = params->dt_init;
+    rc = create_impl(out, &d);
+    if (rc) return rc;
+    setb_handle* h = *out;
+    rc = fl_create(&h->fl, n_cell, n_gran, cell_center, cell_volume, cell_gran, gran_normal, gran_square,
+                   gran_center, gran_neighbour, gran_neighbour_tvd, gran_type, params, h->stream);
+    if (!rc) {
+        clock_reset(h, 0.0);
+        rc = upload_cellpar(h, cell_par);
+    }
+    if (!rc) rc = upload_clock(h);
+    if (rc) {
+        destroy_impl(h);
+        *out = nullptr;
+    }
+    return rc;
+}
+
 int32_t setb_init_cartesian_lism(setb_handle** out, const setb_cart_desc* d, const setb_lism_ic* ic) {
     if (!ic) return SETB_EINVAL;
     int rc = create_impl(out, d);
@@ -399,7 +444,33 @@ int32_t setb_init_cartesian_lism(setb_handle** out, const setb_cart_desc* d, con
 namespace {
 // Enqueues nsteps steps.  When ev is non-null, ev[0..2*nsteps] are recorded before the first
 // launch and after every launch (Euler: ev[2s+1] == ev[2s+2] bracket nothing).
+// Face-list steps: same stage sequence and events as the Cartesian path, three launches per stage.
+int enqueue_fl_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaEvent_t* ev) {
+    if (o->precision != 0) return SETB_EINVAL;
+    h->comp_clean = false;
+    if (ev) SB_TRY(cudaEventRecord(ev[0], h->stream));
+    for (int s = 0; s < nsteps; s++) {
+        double* U = h->buf[h->cur];
+        double* W = h->buf[1 - h->cur];
+        if (o->scheme == 2) {
+            SB_TRY(fl_launch_stage(h->fl, U, nullptr, W, h->g.vs, h->clk, h->st, o, 0, true, false, h->stream));
+            if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
+            SB_TRY(fl_launch_stage(h->fl, W, U, U, h->g.vs, h->clk, h->st, o, 1, false, true, h->stream));
+            if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
+        } else {
+            SB_TRY(fl_launch_stage(h->fl, U, nullptr, W, h->g.vs, h->clk, h->st, o, 0, true, true, h->stream));
+            if (ev) {
+                SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
+                SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
+            }
+            h->cur = 1 - h->cur;
+        }
+    }
+    return SETB_OK;
+}
+
 int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaEvent_t* ev) {
+    if (h->fl) return enqueue_fl_steps(h, nsteps, o, ev);
     StageArgs a{};
     a.g = h->g;
     const int P = o->precision;

@@ -1,0 +1,426 @@
+// facelist.cu -- the MHD step on the reference's own geometry: an explicit face list.
+//
+// The reference's GPU solver (SET_Fortran_Cuda_MHD/cuf_solvers.cuf) runs on an unstructured grid
+// of cells and faces read from the grid file (Storage_module.f90:20-37): a face kernel
+// (CUF_MGD_grans_RK2, :243-440) computes each face's flux once into Gran_POTOK and a cell kernel
+// (CUF_MGD_cell_RK2, :561-794) sums the fluxes of its faces with the owner sign.  This file keeps
+// that structure, B200-side:
+//   * the cell state is conserved SoA FP64 (coalesced in the cell kernel); each stage starts
+//     with a pass that writes the primitive state cell-major (8 doubles = 64 B per cell), so a
+//     face gathers a cell with four 16-byte loads;
+//   * per-face geometry the face kernel needs (the four TVD distances, the reference's "skip"
+//     rule) is derived once at set-up, in the same FP64 arithmetic as the reference's per-step
+//     computation, so the stage kernels read it instead of recomputing it from cell centres;
+//   * the face kernel reduces the dt candidate with warp shuffles and one atomicMin per block;
+//     the cell kernel's last block rolls the lagged-dt clock on the device, so a run of steps
+//     needs no host round trip;
+//   * the face flux array persists between stages: a skipped face keeps its previous flux, as
+//     Gran_POTOK does in the reference.
+// The cell update is the conservative ideal-MHD update of all 8 variables used by the Cartesian
+// path (the reference's live cell kernel is a 2D axisymmetric hydro update; its geometric and
+// charge-exchange sources are not part of this path).
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "setb200.h"
+#include "setb_internal.cuh"
+
+namespace sb {
+
+struct FaceListDev {
+    int64_t n_cell = 0, n_gran = 0;
+    // cells
+    double* cell_center = nullptr;   // [N][3]
+    double* cell_volume = nullptr;   // [N]
+    int32_t* cell_gran = nullptr;    // [N][6], 1-based face numbers, 0 = none
+    unsigned char* cell_flag = nullptr;   // bit 0: frozen (not updated)
+    // faces
+    double* normal = nullptr;        // [G][3]
+    double* square = nullptr;        // [G]
+    double* geo = nullptr;           // [G][4]: dist = |c_face - c_s1|, df2, dff1, dff2
+    int32_t* nb = nullptr;           // [G][2], 1-based, -1 = none
+    int32_t* nbt = nullptr;          // [G][2], 1-based, -1 = none
+    int32_t* type = nullptr;         // [G]: 0 = skipped, else the reference's face type 1..5
+    // work
+    double* prim = nullptr;          // [N][8] primitive state of the stage input
+    double* flux = nullptr;          // [G][8] face flux * area (persistent)
+    GridGeom src{};                  // source-sphere parameters (r_src 0 = none)
+};
+
+namespace {
+
+constexpr int kFaceThreads = 128, kCellThreads = 256, kPrimThreads = 256;
+
+double norm3(const double* x) {
+    return std::sqrt((x[0] * x[0] + x[1] * x[1]) + x[2] * x[2]);
+}
+
+template <typename T>
+cudaError_t upload(T** dst, const T* src, size_t n, cudaStream_t s) {
+    cudaError_t e = cudaMalloc(dst, sizeof(T) * std::max<size_t>(n, 1));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice, s);
+}
+
+// ------------------------------------------------------------------------------ kernels
+__global__ void fl_prim_kernel(int64_t n, const double* __restrict__ U, int64_t vs, double* __restrict__ P) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        double u8[8], q[8], ke, me;
+#pragma unroll
+        for (int v = 0; v < 8; v++) u8[v] = U[v * vs + c];
+        prim_from_cons(u8, q, ke, me);
+        double2* p2 = reinterpret_cast<double2*>(P + 8 * c);
+#pragma unroll
+        for (int v = 0; v < 4; v++) p2[v] = make_double2(q[2 * v], q[2 * v + 1]);
+    }
+}
+
+// Solvers.f90:141-150 at y = 0: linear(x1,t1,x2,t2,x3,t3,0) = minmod of the two one-sided
+// slopes times (0 - x2), plus t2 (IEEE divisions, no contraction, as the reference rounds it).
+__device__ __forceinline__ double linear_ref(double x1, double t1, double x2, double t2, double x3, double t3) {
+    const double d = minmod(__ddiv_rn(dsub(t1, t2), dsub(x1, x2)), __ddiv_rn(dsub(t2, t3), dsub(x2, x3)));
+    return dadd(dmul(d, dsub(0.0, x2)), t2);
+}
+
+__device__ __forceinline__ void load_prim(const double* P, int64_t c, double* q) {
+    const double2* p2 = reinterpret_cast<const double2*>(P + 8 * c);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        const double2 d = __ldg(p2 + v);
+        q[2 * v] = d.x;
+        q[2 * v + 1] = d.y;
+    }
+}
+
+// One face per thread, cuf_solvers.cuf:243-440 (face speed 0).
+template <int NSTATE, int ORDER, bool WANT_DT>
+__global__ void __launch_bounds__(kFaceThreads) fl_face_kernel(const FaceListDev m, double cfl, int n_disc,
+                                                               DevClock* clk, DevStatus* st) {
+    __shared__ double red[kFaceThreads / 32];
+    __shared__ unsigned long long cnt[2];
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t gr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double cand = kDtReset;
+    unsigned n_recon = 0, n_wave = 0;
+    const int type = gr < m.n_gran ? m.type[gr] : 0;
+    if (type != 0) {
+        const int64_t s1 = m.nb[2 * gr] - 1;
+        const int32_t s2r = m.nb[2 * gr + 1];
+        const double n[3] = {m.normal[3 * gr], m.normal[3 * gr + 1], m.normal[3 * gr + 2]};
+        double q1[8], q2[8];
+        load_prim(m.prim, s1, q1);
+        bool tvd = ORDER == 2;
+        if (type == 4) {                          // :318-324 outer boundary
+#pragma unroll
+            for (int v = 0; v < 8; v++) q2[v] = q1[v];
+            if (q2[1] > -0.1) q2[1] = -0.1;
+            tvd = false;
+        } else if (type == 5) {                   // :325-329 axis
+#pragma unroll
+            for (int v = 0; v < 8; v++) q2[v] = q1[v];
+            q2[2] = -q2[2];
+            tvd = false;
+        } else if (type == 2 && s2r == -1) {      // :330-345 reflecting wall
+            const double vel = dadd(dadd(dmul(n[0], q1[1]), dmul(n[1], q1[2])), dmul(n[2], q1[3]));
+#pragma unroll
+            for (int v = 0; v < 8; v++) q2[v] = q1[v];
+#pragma unroll
+            for (int a = 0; a < 3; a++) q2[1 + a] = dsub(dsub(q1[1 + a], dmul(vel, n[a])), dmul(vel, n[a]));
+            tvd = false;
+        } else {
+            load_prim(m.prim, (int64_t)s2r - 1, q2);
+        }
+        const int32_t ss1 = m.nbt[2 * gr], ss2 = m.nbt[2 * gr + 1];
+        const double dist = m.geo[4 * gr];
+        if (tvd && ss1 >= 1 && ss2 >= 1) {       // :358-412, linear on the precomputed distances
+            const double df1 = dist, df2 = m.geo[4 * gr + 1], dff1 = m.geo[4 * gr + 2], dff2 = m.geo[4 * gr + 3];
+            double q11[8], q22[8];
+            load_prim(m.prim, (int64_t)ss1 - 1, q11);
+            load_prim(m.prim, (int64_t)ss2 - 1, q22);
+            double t1[5], t2[5];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                t1[v] = linear_ref(-dff1, q11[v], -df1, q1[v], df2, q2[v]);
+                t2[v] = linear_ref(-dff2, q22[v], -df2, q2[v], df1, q1[v]);
+            }
+            if (t1[0] < 0.0) t1[0] = q1[0];
+            if (t1[4] < 0.0) t1[4] = q1[4];
+            if (t2[0] < 0.0) t2[0] = q2[0];
+            if (t2[4] < 0.0) t2[4] = q2[4];
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                q1[v] = t1[v];
+                q2[v] = t2[v];
+            }
+        }
+        if (q1[0] < 0.0 || q2[0] < 0.0) n_recon++;
+        double qqq[8], sp[3];
+        int32_t fl = 0;
+        chlld_general<double, NSTATE>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);
+        if (fl & kFlagWave) {
+            n_wave++;
+#pragma unroll
+            for (int v = 0; v < 8; v++) qqq[v] = 0.0;
+        }
+        const double sq = m.square[gr];
+        double2* f2 = reinterpret_cast<double2*>(m.flux + 8 * gr);
+#pragma unroll
+        for (int v = 0; v < 4; v++) f2[v] = make_double2(qqq[2 * v] * sq, qqq[2 * v + 1] * sq);
+        if (WANT_DT) cand = fmin(kDtFaceCap, cfl * dist / fmax(fabs(sp[0]), fabs(sp[1])));
+    }
+    if (n_recon) atomicAdd(&cnt[0], (unsigned long long)n_recon);
+    if (n_wave) atomicAdd(&cnt[1], (unsigned long long)n_wave);
+    if (WANT_DT) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cand = fmin(cand, __shfl_xor_sync(0xffffffffu, cand, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = cand;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (WANT_DT) {
+            double r = red[0];
+#pragma unroll
+            for (int w = 1; w < kFaceThreads / 32; w++) r = fmin(r, red[w]);
+            atomicMin(&clk->dt_next, (unsigned long long)__double_as_longlong(r));
+        }
+        if (cnt[0]) atomicAdd(&st->n_recon, cnt[0]);
+        if (cnt[1]) atomicAdd(&st->n_wave, cnt[1]);
+    }
+}
+
+// One cell per thread, cuf_solvers.cuf:561-794 as the conservative MHD update: owner-signed sum
+// of the face fluxes (:691-703), Euler / Heun stage (:705-770), negative-density check, p floor
+// (:777-779), frozen cells (:611) and the re-imposed source sphere.  The last block of a
+// finalizing launch rolls the clock.
+template <int KIND>
+__global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev m, const double* __restrict__ Uin,
+                                                               const double* Ubase, double* Uout, int64_t vs,
+                                                               DevClock* clk, DevStatus* st, int finalize) {
+    __shared__ unsigned long long cnt[2];
+    __shared__ bool last;
+    if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const double dt = clk->dt_cur;
+    if (c < m.n_cell) {
+        double un[8], qs[8];
+        const double x = m.cell_center[3 * c], y = m.cell_center[3 * c + 1], z = m.cell_center[3 * c + 2];
+        const double r2 = dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
+        if (m.cell_flag[c] & 1) {
+#pragma unroll
+            for (int v = 0; v < 8; v++) un[v] = KIND == 0 ? Uin[v * vs + c] : Ubase[v * vs + c];
+        } else if (m.src.r_src > 0.0 && r2 < dmul(m.src.r_src, m.src.r_src)) {
+            source_state(m.src, x, y, z, r2, qs);
+            cons_from_prim_exact(qs, un);
+        } else {
+            double pot[8];
+#pragma unroll
+            for (int v = 0; v < 8; v++) pot[v] = 0.0;
+            for (int f = 0; f < 6; f++) {
+                const int32_t j = m.cell_gran[6 * c + f];
+                if (j == 0) continue;
+                const int64_t jf = (int64_t)j - 1;
+                const bool owner = m.nb[2 * jf] == (int32_t)(c + 1);
+                const double2* f2 = reinterpret_cast<const double2*>(m.flux + 8 * jf);
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    const double2 d = f2[v];
+                    pot[2 * v] = owner ? pot[2 * v] + d.x : pot[2 * v] - d.x;
+                    pot[2 * v + 1] = owner ? pot[2 * v + 1] + d.y : pot[2 * v + 1] - d.y;
+                }
+            }
+            const double vol = m.cell_volume[c];
+            double uin[8];
+#pragma unroll
+            for (int v = 0; v < 8; v++) {
+                uin[v] = Uin[v * vs + c];
+                if (KIND == 0) un[v] = uin[v] - dt * (pot[v] / vol);
+                else un[v] = 0.5 * ((Ubase[v * vs + c] + uin[v]) - dt * (pot[v] / vol));
+            }
+            if (!(un[0] > 0.0)) {
+                atomicAdd(&cnt[0], 1ull);
+                atomicMin(&st->first_bad, (unsigned long long)c);
+#pragma unroll
+                for (int v = 0; v < 8; v++) un[v] = uin[v];
+            } else {
+                double q[8], ke, me;
+                prim_from_cons(un, q, ke, me);
+                if (q[4] <= 0.0) {
+                    atomicAdd(&cnt[1], 1ull);
+                    un[4] = (kPFloor * kInvG1 + ke) + me;
+                }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < 8; v++) Uout[v * vs + c] = un[v];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (cnt[0]) atomicAdd(&st->n_negdens, cnt[0]);
+        if (cnt[1]) atomicAdd(&st->n_pfloor, cnt[1]);
+        __threadfence();
+        last = atomicAdd(&clk->counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        clk->counter = 0;
+        if (finalize) {
+            const unsigned long long nb = atomicExch(&clk->dt_next, (unsigned long long)__double_as_longlong(kDtReset));
+            clk->time_all += clk->dt_cur;
+            clk->dt_last = clk->dt_cur;
+            clk->dt_cur = __longlong_as_double((long long)nb);
+            clk->steps += 1;
+        }
+        __threadfence();
+    }
+}
+
+template <int NSTATE>
+void launch_face_n(const FaceListDev& m, int order, bool want_dt, double cfl, int n_disc, DevClock* clk,
+                   DevStatus* st, cudaStream_t s) {
+    const unsigned grid = (unsigned)((m.n_gran + kFaceThreads - 1) / kFaceThreads);
+    if (order == 2) {
+        if (want_dt) fl_face_kernel<NSTATE, 2, true><<<grid, kFaceThreads, 0, s>>>(m, cfl, n_disc, clk, st);
+        else fl_face_kernel<NSTATE, 2, false><<<grid, kFaceThreads, 0, s>>>(m, cfl, n_disc, clk, st);
+    } else {
+        if (want_dt) fl_face_kernel<NSTATE, 1, true><<<grid, kFaceThreads, 0, s>>>(m, cfl, n_disc, clk, st);
+        else fl_face_kernel<NSTATE, 1, false><<<grid, kFaceThreads, 0, s>>>(m, cfl, n_disc, clk, st);
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------ host side
+void fl_destroy(FaceListDev* f) {
+    if (!f) return;
+    void* ptrs[] = {f->cell_center, f->cell_volume, f->cell_gran, f->cell_flag, f->normal, f->square,
+                    f->geo,         f->nb,          f->nbt,       f->type,      f->prim,   f->flux};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete f;
+}
+
+// Host-side check that every index the kernels follow stays inside its array: cell faces in
+// 0..G, neighbours in 1..N (neighbour 2 may be -1 only on a ghost face: type 4, 5, or a type-2
+// wall), TVD cells in 1..N or -1, face types 1..5, volumes positive.
+int fl_validate(int64_t N, int64_t G, const double* cell_center, const double* cell_volume, const int32_t* cell_gran,
+                const double* gran_normal, const double* gran_square, const double* gran_center,
+                const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd, const int32_t* gran_type) {
+    if (N < 1 || G < 1 || !cell_center || !cell_volume || !cell_gran || !gran_normal || !gran_square || !gran_center ||
+        !gran_neighbour || !gran_neighbour_tvd || !gran_type)
+        return SETB_EINVAL;
+    if (N > INT32_MAX - 1 || G > INT32_MAX - 1) return SETB_ESIZE;
+    for (int64_t c = 0; c < N; c++) {
+        if (!(cell_volume[c] > 0.0)) return SETB_EINVAL;
+        for (int f = 0; f < 6; f++) {
+            const int32_t j = cell_gran[6 * c + f];
+            if (j < 0 || j > G) return SETB_EINVAL;
+        }
+    }
+    for (int64_t g = 0; g < G; g++) {
+        const int32_t s1 = gran_neighbour[2 * g], s2 = gran_neighbour[2 * g + 1], t = gran_type[g];
+        const int32_t ss1 = gran_neighbour_tvd[2 * g], ss2 = gran_neighbour_tvd[2 * g + 1];
+        if (s1 < 1 || s1 > N || t < 1 || t > 5) return SETB_EINVAL;
+        const bool ghost = t == 4 || t == 5 || (t == 2 && s2 == -1);
+        if (!ghost && (s2 < 1 || s2 > N)) return SETB_EINVAL;
+        if ((ss1 != -1 && (ss1 < 1 || ss1 > N)) || (ss2 != -1 && (ss2 < 1 || ss2 > N))) return SETB_EINVAL;
+    }
+    return SETB_OK;
+}
+
+int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center, const double* cell_volume,
+              const int32_t* cell_gran, const double* gran_normal, const double* gran_square,
+              const double* gran_center, const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd,
+              const int32_t* gran_type, const setb_fl_params* p, cudaStream_t s) {
+    *out = nullptr;
+    if (!p) return SETB_EINVAL;
+    int rc = fl_validate(N, G, cell_center, cell_volume, cell_gran, gran_normal, gran_square, gran_center,
+                         gran_neighbour, gran_neighbour_tvd, gran_type);
+    if (rc) return rc;
+    std::vector<double> geo((size_t)G * 4);
+    std::vector<int32_t> type((size_t)G);
+    for (int64_t g = 0; g < G; g++) {
+        const int32_t s1 = gran_neighbour[2 * g], s2 = gran_neighbour[2 * g + 1];
+        const int32_t t = gran_type[g];
+        const int32_t ss1 = gran_neighbour_tvd[2 * g], ss2 = gran_neighbour_tvd[2 * g + 1];
+        const bool ghost = t == 4 || t == 5 || (t == 2 && s2 == -1);
+        // distances as the reference forms them each step (cuf_solvers.cuf:290-292, 362-372)
+        const double* gc = gran_center + 3 * g;
+        const double* c1 = cell_center + 3 * (int64_t)(s1 - 1);
+        const double* c2 = ghost ? c1 : cell_center + 3 * (int64_t)(s2 - 1);
+        double r[3];
+        for (int a = 0; a < 3; a++) r[a] = gc[a] - c1[a];
+        geo[4 * g] = norm3(r);
+        for (int a = 0; a < 3; a++) r[a] = gc[a] - c2[a];
+        geo[4 * g + 1] = norm3(r);
+        geo[4 * g + 2] = geo[4 * g + 3] = 0.0;
+        if (ss1 >= 1) {
+            for (int a = 0; a < 3; a++) r[a] = gc[a] - cell_center[3 * (int64_t)(ss1 - 1) + a];
+            geo[4 * g + 2] = norm3(r);
+        }
+        if (ss2 >= 1) {
+            for (int a = 0; a < 3; a++) r[a] = gc[a] - cell_center[3 * (int64_t)(ss2 - 1) + a];
+            geo[4 * g + 3] = norm3(r);
+        }
+        // the reference skips faces whose first cell lies inside its frozen core (:284)
+        type[g] = (p->face_skip_radius > 0.0 && norm3(c1) < p->face_skip_radius) ? 0 : t;
+    }
+    std::vector<unsigned char> flag((size_t)N);
+    for (int64_t c = 0; c < N; c++)
+        flag[c] = (p->cell_freeze_radius > 0.0 && norm3(cell_center + 3 * c) < p->cell_freeze_radius) ? 1 : 0;
+
+    FaceListDev* f = new (std::nothrow) FaceListDev();
+    if (!f) return SETB_ENOMEM;
+    f->n_cell = N;
+    f->n_gran = G;
+    f->src.r_src = p->r_src;
+    f->src.rho_src = p->rho_src;
+    f->src.v_src = p->v_src;
+    f->src.p_over_rho_src = p->p_over_rho_src;
+    f->src.r_floor = p->r_floor;
+    bool ok = upload(&f->cell_center, cell_center, 3 * (size_t)N, s) == cudaSuccess &&
+              upload(&f->cell_volume, cell_volume, (size_t)N, s) == cudaSuccess &&
+              upload(&f->cell_gran, cell_gran, 6 * (size_t)N, s) == cudaSuccess &&
+              upload(&f->cell_flag, flag.data(), (size_t)N, s) == cudaSuccess &&
+              upload(&f->normal, gran_normal, 3 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->square, gran_square, (size_t)G, s) == cudaSuccess &&
+              upload(&f->geo, geo.data(), 4 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->nb, gran_neighbour, 2 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->nbt, gran_neighbour_tvd, 2 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->type, type.data(), (size_t)G, s) == cudaSuccess &&
+              cudaMalloc(&f->prim, sizeof(double) * 8 * (size_t)N) == cudaSuccess &&
+              cudaMalloc(&f->flux, sizeof(double) * 8 * (size_t)G) == cudaSuccess &&
+              cudaMemsetAsync(f->flux, 0, sizeof(double) * 8 * (size_t)G, s) == cudaSuccess &&
+              cudaStreamSynchronize(s) == cudaSuccess;   // host vectors are released on return
+    if (!ok) {
+        cudaGetLastError();
+        fl_destroy(f);
+        return SETB_ENOMEM;
+    }
+    *out = f;
+    return SETB_OK;
+}
+
+cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const double* Ubase, double* Uout, int64_t vs,
+                            DevClock* clk, DevStatus* st, const setb_step_opts* o, int kind, bool want_dt,
+                            bool finalize, cudaStream_t s) {
+    const FaceListDev& m = *f;
+    const unsigned pgrid = (unsigned)std::min<int64_t>((m.n_cell + kPrimThreads - 1) / kPrimThreads, 148 * 16);
+    fl_prim_kernel<<<pgrid, kPrimThreads, 0, s>>>(m.n_cell, Uin, vs, m.prim);
+    switch (o->n_state) {
+        case 0: launch_face_n<0>(m, o->order, want_dt, o->cfl, o->n_disc, clk, st, s); break;
+        case 1: launch_face_n<1>(m, o->order, want_dt, o->cfl, o->n_disc, clk, st, s); break;
+        case 2: launch_face_n<2>(m, o->order, want_dt, o->cfl, o->n_disc, clk, st, s); break;
+        default: launch_face_n<3>(m, o->order, want_dt, o->cfl, o->n_disc, clk, st, s); break;
+    }
+    const unsigned cgrid = (unsigned)((m.n_cell + kCellThreads - 1) / kCellThreads);
+    if (kind == 0) fl_cell_kernel<0><<<cgrid, kCellThreads, 0, s>>>(m, Uin, Ubase, Uout, vs, clk, st, finalize);
+    else fl_cell_kernel<1><<<cgrid, kCellThreads, 0, s>>>(m, Uin, Ubase, Uout, vs, clk, st, finalize);
+    return cudaGetLastError();
+}
+
+}  // namespace sb

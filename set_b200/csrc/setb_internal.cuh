@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include "mhd_core.cuh"
+#include "setb200.h"
 
 namespace sb {
 
@@ -306,6 +307,22 @@ inline void set_device_strides(GridGeom& g) {
 // g, box (kTileX + 4, tile_shape(precision).ty + 4, 1, 8): one plane of a column tile with its
 // 2-cell halo.  Returns a SETB_* status.
 int encode_state_tmap(const GridGeom& g, const double* base, int precision, CUtensorMap* out);
+
+// ---------------------------------------------------------------- face-list grids (facelist.cu)
+struct FaceListDev;
+int fl_validate(int64_t N, int64_t G, const double* cell_center, const double* cell_volume, const int32_t* cell_gran,
+                const double* gran_normal, const double* gran_square, const double* gran_center,
+                const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd, const int32_t* gran_type);
+int fl_create(FaceListDev** out, int64_t n_cell, int64_t n_gran, const double* cell_center, const double* cell_volume,
+              const int32_t* cell_gran, const double* gran_normal, const double* gran_square,
+              const double* gran_center, const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd,
+              const int32_t* gran_type, const setb_fl_params* p, cudaStream_t s);
+void fl_destroy(FaceListDev* f);
+// One stage on the face list: primitive pass, face fluxes (+ dt candidate when want_dt), cell
+// update (kind 0: Euler / Heun stage 1, kind 1: Heun stage 2); a finalizing stage rolls the clock.
+cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const double* Ubase, double* Uout, int64_t vs,
+                            DevClock* clk, DevStatus* st, const setb_step_opts* o, int kind, bool want_dt,
+                            bool finalize, cudaStream_t s);
 
 // ---------------------------------------------------------------- launch entry points
 cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int kind, bool want_dt,

@@ -1,0 +1,118 @@
+"""Face-list grids on the CPU: the generator's connectivity, the oracle's face-list driver
+(properties the reference's face/cell kernels imply: numbering does not matter, walls conserve
+mass -- and energy without a field --, a state at rest stays at rest) and the C ABI's host-side
+mesh validation."""
+import numpy as np
+import pytest
+
+import oracle as O
+import set_b200 as S
+from set_b200 import facelist as FL
+
+
+def check_connectivity(m):
+    N, G = m.n_cell, m.n_gran
+    cnt = np.zeros(G, int)
+    for c in range(N):
+        for f in m.cell_gran[c]:
+            if f == 0:
+                continue
+            assert 1 <= f <= G
+            assert c + 1 in tuple(m.gran_neighbour[f - 1])
+            cnt[f - 1] += 1
+    inner = m.gran_neighbour[:, 1] > 0
+    assert np.all(cnt[inner] == 2) and np.all(cnt[~inner] == 1)
+    d = m.cell_center[m.gran_neighbour[inner, 1] - 1] - m.cell_center[m.gran_neighbour[inner, 0] - 1]
+    assert np.all((d * m.gran_normal[inner]).sum(1) > 0)
+    d = m.gran_center[~inner] - m.cell_center[m.gran_neighbour[~inner, 0] - 1]
+    assert np.all((d * m.gran_normal[~inner]).sum(1) > 0)
+
+
+@pytest.mark.parametrize("shape,stretch,perm", [((5, 4, 3), 0.0, None), ((6, 5, 4), 0.6, 7)])
+def test_box_facelist_connectivity(shape, stretch, perm):
+    m = FL.box_facelist(shape, stretch=stretch, permute_seed=perm, seed=2)
+    nx, ny, nz = shape
+    assert m.n_cell == nx * ny * nz
+    assert m.n_gran == (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+    assert abs(m.cell_volume.sum() - 8.0) < 1e-12
+    check_connectivity(m)
+
+
+def run_oracle(m, params, cp, opts, nsteps):
+    om = O.facelist(m, params)
+    U = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1).copy()
+    ck, dg, _ = O.fl_run(om, opts, U, nsteps)
+    return U, ck, dg
+
+
+def test_oracle_facelist_numbering_does_not_matter():
+    params = FL.fl_params(r_src=0.5, rho_src=5.0, dt_init=1e-3)
+    a = FL.box_facelist((7, 6, 5), stretch=0.4, seed=3)
+    b = FL.box_facelist((7, 6, 5), stretch=0.4, seed=3, permute_seed=11)
+    cpa = FL.lism_cellpar(a, seed=5, params=params)
+    # the same physical cell in b: match by centre
+    key = lambda x: np.lexsort((x[:, 0], x[:, 1], x[:, 2]))
+    ia, ib = key(a.cell_center), key(b.cell_center)
+    cpb = np.zeros_like(cpa)
+    cpb[ib] = cpa[ia]
+    o = O.make_opts(3, 2, 2, 0.4)
+    Ua, cka, _ = run_oracle(a, params, cpa, o, 6)
+    Ub, ckb, _ = run_oracle(b, params, cpb, o, 6)
+    assert np.array_equal(Ua[:, ia], Ub[:, ib])
+    assert cka.time_all == ckb.time_all
+
+
+@pytest.mark.parametrize("n_state", [2, 3])
+def test_oracle_facelist_walls_conserve(n_state):
+    walls = {k: 2 for k in ("x-", "x+", "y-", "y+", "z-", "z+")}
+    m = FL.box_facelist((6, 5, 4), stretch=0.5, sides=walls, seed=1, permute_seed=3)
+    params = FL.fl_params(r_src=0.0, dt_init=1e-3)
+    cp = FL.lism_cellpar(m, seed=2, pert_amp=0.2)
+    if n_state == 2:
+        cp[:, 5:8] = 0.0
+    U0 = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1)
+    U, ck, dg = run_oracle(m, params, cp, O.make_opts(n_state, 2, 2, 0.4), 10)
+    vol = m.cell_volume
+    # the reference's wall mirrors the velocity only, so with a field the Poynting flux crosses it:
+    # mass is conserved in both cases, energy in the hydro case
+    for v in ((0, 4) if n_state == 2 else (0,)):
+        tot0, tot = (U0[v] * vol).sum(), (U[v] * vol).sum()
+        assert abs(tot - tot0) <= 1e-13 * abs(tot0), (v, tot0, tot)
+    assert dg.n_negdens == 0 and dg.n_pfloor == 0
+
+
+def test_oracle_facelist_rest_state_stays():
+    walls = {k: 2 for k in ("x-", "x+", "y-", "y+", "z-", "z+")}
+    m = FL.box_facelist((5, 5, 5), stretch=0.3, sides=walls, seed=4)
+    params = FL.fl_params(r_src=0.0, dt_init=1e-3)
+    cp = FL.lism_cellpar(m, lism=np.array([1.3, 0, 0, 0, 0.7, 0.2, -0.4, 0.1]), pert_amp=0.0)
+    U0 = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1)
+    U, _, _ = run_oracle(m, params, cp, O.make_opts(3, 2, 2, 0.4), 5)
+    assert np.allclose(U, U0, rtol=0, atol=1e-14)
+
+
+def test_init_facelist_validates_on_the_host():
+    m = FL.box_facelist((4, 3, 3), seed=1)
+    params = FL.fl_params()
+    cp = FL.lism_cellpar(m)
+    try:   # a valid mesh passes the host checks: it then needs a device (ENODEV without one)
+        FL.FaceListSolver(m, cp, params).close()
+    except S.SetbError as e:
+        assert e.code == 8, e
+    bad = FL.FaceList(**{k: getattr(m, k).copy() for k in m.__dataclass_fields__})
+    bad.gran_neighbour[5, 0] = m.n_cell + 7          # a cell number outside the grid
+    with pytest.raises(S.SetbError) as e:
+        FL.FaceListSolver(bad, cp, params)
+    assert e.value.code == 1
+    bad = FL.FaceList(**{k: getattr(m, k).copy() for k in m.__dataclass_fields__})
+    bad.gran_type[3] = 9                               # unknown face type
+    with pytest.raises(S.SetbError) as e:
+        FL.FaceListSolver(bad, cp, params)
+    assert e.value.code == 1
+    bad = FL.FaceList(**{k: getattr(m, k).copy() for k in m.__dataclass_fields__})
+    inner = np.where(bad.gran_neighbour[:, 1] > 0)[0][0]
+    bad.gran_neighbour[inner, 1] = -1                  # a missing neighbour on an ordinary face
+    bad.gran_type[inner] = 1
+    with pytest.raises(S.SetbError) as e:
+        FL.FaceListSolver(bad, cp, params)
+    assert e.value.code == 1
