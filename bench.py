@@ -172,6 +172,27 @@ def config_dict(args, reference=False):
             "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single"}
 
 
+def facelist_leg(n: int, tsteps: int, permute: bool):
+    """The face-list path (the reference's own geometry) on an n^3 box of the C2 physics, cells and
+    faces in natural order or renumbered at random: cell-updates/s from CUDA events around every
+    stage (3 launches each), and the DRAM bytes per cell-update a stage needs at least."""
+    from set_b200 import facelist as FL
+    m = FL.box_facelist((n, n, n), seed=1, permute_seed=7 if permute else None,
+                        sides={"x-": 4, "x+": 4, "y-": 4, "y+": 4, "z-": 4, "z+": 4})
+    params = FL.fl_params(r_src=0.125, rho_src=50.0, v_src=10.0, p_over_rho_src=0.01, r_floor=1.0 / n, dt_init=2e-9)
+    cp = FL.lism_cellpar(m, seed=2, params=params)
+    o = __import__("set_b200").step_opts(n_state=3, order=2, scheme=2, cfl=0.4)
+    with FL.FaceListSolver(m, cp, params) as s:
+        s.step(5, o)
+        _, ms, cnt = s.step_profiled(tsteps, o)
+        diag = s.status()
+    cells = m.n_cell
+    return {"grid": f"{n}^3 box, {'random' if permute else 'natural'} numbering", "cells": cells,
+            "faces": m.n_gran, "time_steps": tsteps, "cell_updates_per_s": cells * tsteps / (sum(ms) / 1e3),
+            "stage1_ms": ms[0] / max(cnt[0], 1), "stage2_ms": ms[1] / max(cnt[1], 1),
+            "n_negdens": diag.n_negdens}
+
+
 def run_mixed_only(args):
     """`--mixed-only`: only the mixed-form leg (W warm-up and K timed solves); used to profile the
     mixed kernel in isolation."""
@@ -356,6 +377,11 @@ def run_ours(args, world, rank, local):
                   "sequential_plain_solves_per_s": seq["solves_per_s"],
                   "speedup_vs_sequential_plain": out["solves_per_s"] / seq["solves_per_s"]}
 
+    # ---- the face-list path (SURVEY "next" row: the reference's geometry) on a 128^3 box
+    facelist = None
+    if rank == 0 and world == 1 and args.facelist_n > 0:
+        facelist = [facelist_leg(args.facelist_n, 50, False), facelist_leg(args.facelist_n, 50, True)]
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, thr, secs = cpu_baseline(n)
@@ -381,6 +407,7 @@ def run_ours(args, world, rank, local):
             "mixed": mixed,
             "ensemble": ensemble,
             "served": served,
+            "facelist": facelist,
             "cpu_baseline": base,
             "clocks": clocks,
             "gpu_launches": int(sum(k_n)),
@@ -409,6 +436,7 @@ def main():
                     help="mixed form: 1 FP32 Riemann arithmetic, 2 the delta form")
     ap.add_argument("--c3", type=int, default=0, help="run config C3 (mixed vs plain) on this many seeded draws")
     ap.add_argument("--serve-requests", type=int, default=100)
+    ap.add_argument("--facelist-n", type=int, default=128, help="face-list leg on an n^3 box (0 = off)")
     ap.add_argument("--serve-max-edge", type=int, default=96)
     ap.add_argument("--serve-max-steps", type=int, default=600)
     args = ap.parse_args()

@@ -202,7 +202,9 @@ SETB_API int32_t setb_destroy(setb_handle* h);
  * setb_step_profiled, setb_get_state, setb_set_state, setb_get_conserved, setb_status and
  * setb_destroy like a Cartesian one; it supports precision 0 (plain FP64).  Indices are checked
  * on the host: an index outside its array, a non-positive volume or an unknown face type gives
- * SETB_EINVAL. */
+ * SETB_EINVAL.  The library stores cells in its own locality order (Morton order of the centres,
+ * faces by their first cell); every state transfer and the first-bad-cell index use the
+ * caller's numbering, only setb_state_view exposes the internal order. */
 typedef struct {
     double r_src, rho_src, v_src, p_over_rho_src, r_floor;   /* source sphere, r_src 0 = none  */
     double dt_init;             /* dt of the first step (reference: 2e-9, cuf_kernel.cuf:758)    */

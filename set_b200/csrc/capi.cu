@@ -240,11 +240,21 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
     return SETB_OK;
 }
 
-// Uploads Cell_par columns 1..8 (16 doubles per cell) into buf[cur] through buf[1-cur].
+// Uploads Cell_par columns 1..8 (16 doubles per cell) into buf[cur] through buf[1-cur].  A
+// face-list handle keeps its cells in locality order: row d of the device state is the caller's
+// cell perm[d].
 int upload_cellpar(setb_handle* h, const double* cell_par) {
     h->comp_clean = false;
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
     double* stage = h->buf[1 - h->cur];
+    if (const int32_t* perm = fl_perm(h->fl)) {
+        std::vector<double> tmp(8 * N);
+        for (size_t d = 0; d < N; d++) std::memcpy(&tmp[8 * d], cell_par + 16 * (size_t)perm[d], 8 * sizeof(double));
+        SB_TRY(cudaMemcpyAsync(stage, tmp.data(), sizeof(double) * 8 * N, cudaMemcpyHostToDevice, h->stream));
+        SB_TRY(launch_prim_to_cons(h->g, stage, h->buf[h->cur], h->stream));
+        SB_TRY(cudaStreamSynchronize(h->stream));   // tmp is released on return
+        return SETB_OK;
+    }
     SB_TRY(cudaMemcpy2DAsync(stage, 8 * sizeof(double), cell_par, 16 * sizeof(double), 8 * sizeof(double), N,
                              cudaMemcpyHostToDevice, h->stream));
     SB_TRY(launch_prim_to_cons(h->g, stage, h->buf[h->cur], h->stream));
@@ -605,8 +615,15 @@ int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_all) {
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
     double* stage = h->buf[1 - h->cur];
     SB_TRY(launch_cons_to_prim(h->g, h->buf[h->cur], stage, h->stream));
-    SB_TRY(cudaMemcpy2DAsync(cell_par, 16 * sizeof(double), stage, 8 * sizeof(double), 8 * sizeof(double), N,
-                             cudaMemcpyDeviceToHost, h->stream));
+    if (const int32_t* perm = fl_perm(h->fl)) {
+        std::vector<double> tmp(8 * N);
+        SB_TRY(cudaMemcpyAsync(tmp.data(), stage, sizeof(double) * 8 * N, cudaMemcpyDeviceToHost, h->stream));
+        SB_TRY(cudaStreamSynchronize(h->stream));
+        for (size_t d = 0; d < N; d++) std::memcpy(cell_par + 16 * (size_t)perm[d], &tmp[8 * d], 8 * sizeof(double));
+    } else {
+        SB_TRY(cudaMemcpy2DAsync(cell_par, 16 * sizeof(double), stage, 8 * sizeof(double), 8 * sizeof(double), N,
+                                 cudaMemcpyDeviceToHost, h->stream));
+    }
     int rc = download_clock(h);
     if (rc) return rc;
     if (time_all) *time_all = h->h_clk->time_all;
@@ -651,11 +668,17 @@ int32_t setb_get_conserved(setb_handle* h, double* U) {
     if (!h || !U) return SETB_EINVAL;
     cudaSetDevice(h->device);
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    const int32_t* perm = fl_perm(h->fl);
+    std::vector<double> tmp(perm ? 8 * N : 0);
+    double* dst = perm ? tmp.data() : U;
     for (int v = 0; v < 8; v++)
-        SB_TRY(cudaMemcpy2DAsync(U + v * N, h->g.nx * sizeof(double), h->buf[h->cur] + v * h->g.vs,
+        SB_TRY(cudaMemcpy2DAsync(dst + v * N, h->g.nx * sizeof(double), h->buf[h->cur] + v * h->g.vs,
                                  h->g.px * sizeof(double), h->g.nx * sizeof(double), (size_t)h->g.ny * h->g.nz,
                                  cudaMemcpyDeviceToHost, h->stream));
     SB_TRY(cudaStreamSynchronize(h->stream));
+    if (perm)
+        for (int v = 0; v < 8; v++)
+            for (size_t d = 0; d < N; d++) U[v * N + (size_t)perm[d]] = tmp[v * N + d];
     return SETB_OK;
 }
 
@@ -672,6 +695,7 @@ int32_t setb_status(setb_handle* h, setb_diag* out) {
     out->steps = c.steps;
     out->n_negdens = (int64_t)s.n_negdens;
     out->first_bad_cell = s.first_bad == ULLONG_MAX ? -1 : (int64_t)s.first_bad;
+    if (out->first_bad_cell >= 0 && fl_perm(h->fl)) out->first_bad_cell = fl_perm(h->fl)[out->first_bad_cell];
     out->n_pfloor = (int64_t)s.n_pfloor;
     out->n_wave_err = (int64_t)s.n_wave;
     out->n_recon_err = (int64_t)s.n_recon;

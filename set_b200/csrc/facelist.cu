@@ -19,9 +19,11 @@
 // The cell update is the conservative ideal-MHD update of all 8 variables used by the Cartesian
 // path (the reference's live cell kernel is a 2D axisymmetric hydro update; its geometric and
 // charge-exchange sources are not part of this path).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <numeric>
 #include <vector>
 
 #include "setb200.h"
@@ -47,6 +49,8 @@ struct FaceListDev {
     double* prim = nullptr;          // [N][8] primitive state of the stage input
     double* flux = nullptr;          // [G][8] face flux * area (persistent)
     GridGeom src{};                  // source-sphere parameters (r_src 0 = none)
+    // locality order: device cell d holds the caller's cell perm[d] (both 0-based)
+    std::vector<int32_t> perm;
 };
 
 namespace {
@@ -96,7 +100,7 @@ __device__ __forceinline__ void load_prim(const double* P, int64_t c, double* q)
 
 // One face per thread, cuf_solvers.cuf:243-440 (face speed 0).
 template <int NSTATE, int ORDER, bool WANT_DT>
-__global__ void __launch_bounds__(kFaceThreads) fl_face_kernel(const FaceListDev m, double cfl, int n_disc,
+__global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceListDev m, double cfl, int n_disc,
                                                                DevClock* clk, DevStatus* st) {
     __shared__ double red[kFaceThreads / 32];
     __shared__ unsigned long long cnt[2];
@@ -332,15 +336,86 @@ int fl_validate(int64_t N, int64_t G, const double* cell_center, const double* c
     return SETB_OK;
 }
 
-int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center, const double* cell_volume,
-              const int32_t* cell_gran, const double* gran_normal, const double* gran_square,
-              const double* gran_center, const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd,
-              const int32_t* gran_type, const setb_fl_params* p, cudaStream_t s) {
+namespace {
+// 21-bit spread for a 63-bit Morton code
+uint64_t spread3(uint64_t x) {
+    x &= 0x1fffffull;
+    x = (x | x << 32) & 0x1f00000000ffffull;
+    x = (x | x << 16) & 0x1f0000ff0000ffull;
+    x = (x | x << 8) & 0x100f00f00f00f00full;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+    x = (x | x << 2) & 0x1249249249249249ull;
+    return x;
+}
+}  // namespace
+
+int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center_in, const double* cell_volume_in,
+              const int32_t* cell_gran_in, const double* gran_normal_in, const double* gran_square_in,
+              const double* gran_center_in, const int32_t* gran_neighbour_in, const int32_t* gran_neighbour_tvd_in,
+              const int32_t* gran_type_in, const setb_fl_params* p, cudaStream_t s) {
     *out = nullptr;
     if (!p) return SETB_EINVAL;
-    int rc = fl_validate(N, G, cell_center, cell_volume, cell_gran, gran_normal, gran_square, gran_center,
-                         gran_neighbour, gran_neighbour_tvd, gran_type);
+    int rc = fl_validate(N, G, cell_center_in, cell_volume_in, cell_gran_in, gran_normal_in, gran_square_in,
+                         gran_center_in, gran_neighbour_in, gran_neighbour_tvd_in, gran_type_in);
     if (rc) return rc;
+    // Locality order: cells along the Morton curve of their centres, faces by their first cell, so
+    // the cells a face gathers and the faces a cell gathers sit close in memory whatever the
+    // caller's numbering.  cperm[d] = caller's cell of device cell d; fperm likewise for faces.
+    std::vector<int32_t> cperm((size_t)N), fperm((size_t)G), cnew((size_t)N), fnew((size_t)G);
+    {
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int64_t c = 0; c < N; c++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = std::min(lo[a], cell_center_in[3 * c + a]);
+                hi[a] = std::max(hi[a], cell_center_in[3 * c + a]);
+            }
+        std::vector<uint64_t> key((size_t)N);
+        for (int64_t c = 0; c < N; c++) {
+            uint64_t code = 0;
+            for (int a = 0; a < 3; a++) {
+                const double span = hi[a] > lo[a] ? hi[a] - lo[a] : 1.0;
+                const double u = (cell_center_in[3 * c + a] - lo[a]) / span;
+                code |= spread3((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << a;
+            }
+            key[c] = code;
+        }
+        std::iota(cperm.begin(), cperm.end(), 0);
+        std::stable_sort(cperm.begin(), cperm.end(), [&](int32_t x, int32_t y) { return key[x] < key[y]; });
+        for (int64_t d = 0; d < N; d++) cnew[cperm[d]] = (int32_t)d;
+        std::iota(fperm.begin(), fperm.end(), 0);
+        std::stable_sort(fperm.begin(), fperm.end(), [&](int32_t x, int32_t y) {
+            return cnew[gran_neighbour_in[2 * (int64_t)x] - 1] < cnew[gran_neighbour_in[2 * (int64_t)y] - 1];
+        });
+        for (int64_t d = 0; d < G; d++) fnew[fperm[d]] = (int32_t)d;
+    }
+    auto cell_ref = [&](int32_t c1) { return c1 >= 1 ? cnew[c1 - 1] + 1 : c1; };   // 1-based, -1 kept
+    std::vector<double> cell_center((size_t)N * 3), cell_volume((size_t)N), gran_normal((size_t)G * 3),
+        gran_square((size_t)G), gran_center((size_t)G * 3);
+    std::vector<int32_t> cell_gran((size_t)N * 6), gran_neighbour((size_t)G * 2), gran_neighbour_tvd((size_t)G * 2),
+        gran_type_v((size_t)G);
+    for (int64_t d = 0; d < N; d++) {
+        const int64_t c = cperm[d];
+        for (int a = 0; a < 3; a++) cell_center[3 * d + a] = cell_center_in[3 * c + a];
+        cell_volume[d] = cell_volume_in[c];
+        for (int f = 0; f < 6; f++) {
+            const int32_t j = cell_gran_in[6 * c + f];
+            cell_gran[6 * d + f] = j >= 1 ? fnew[j - 1] + 1 : 0;
+        }
+    }
+    for (int64_t d = 0; d < G; d++) {
+        const int64_t g = fperm[d];
+        for (int a = 0; a < 3; a++) {
+            gran_normal[3 * d + a] = gran_normal_in[3 * g + a];
+            gran_center[3 * d + a] = gran_center_in[3 * g + a];
+        }
+        gran_square[d] = gran_square_in[g];
+        for (int b = 0; b < 2; b++) {
+            gran_neighbour[2 * d + b] = cell_ref(gran_neighbour_in[2 * g + b]);
+            gran_neighbour_tvd[2 * d + b] = cell_ref(gran_neighbour_tvd_in[2 * g + b]);
+        }
+        gran_type_v[d] = gran_type_in[g];
+    }
+    const int32_t* gran_type = gran_type_v.data();
     std::vector<double> geo((size_t)G * 4);
     std::vector<int32_t> type((size_t)G);
     for (int64_t g = 0; g < G; g++) {
@@ -349,9 +424,9 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
         const int32_t ss1 = gran_neighbour_tvd[2 * g], ss2 = gran_neighbour_tvd[2 * g + 1];
         const bool ghost = t == 4 || t == 5 || (t == 2 && s2 == -1);
         // distances as the reference forms them each step (cuf_solvers.cuf:290-292, 362-372)
-        const double* gc = gran_center + 3 * g;
-        const double* c1 = cell_center + 3 * (int64_t)(s1 - 1);
-        const double* c2 = ghost ? c1 : cell_center + 3 * (int64_t)(s2 - 1);
+        const double* gc = gran_center.data() + 3 * g;
+        const double* c1 = cell_center.data() + 3 * (int64_t)(s1 - 1);
+        const double* c2 = ghost ? c1 : cell_center.data() + 3 * (int64_t)(s2 - 1);
         double r[3];
         for (int a = 0; a < 3; a++) r[a] = gc[a] - c1[a];
         geo[4 * g] = norm3(r);
@@ -371,7 +446,7 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
     }
     std::vector<unsigned char> flag((size_t)N);
     for (int64_t c = 0; c < N; c++)
-        flag[c] = (p->cell_freeze_radius > 0.0 && norm3(cell_center + 3 * c) < p->cell_freeze_radius) ? 1 : 0;
+        flag[c] = (p->cell_freeze_radius > 0.0 && norm3(cell_center.data() + 3 * c) < p->cell_freeze_radius) ? 1 : 0;
 
     FaceListDev* f = new (std::nothrow) FaceListDev();
     if (!f) return SETB_ENOMEM;
@@ -382,15 +457,16 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
     f->src.v_src = p->v_src;
     f->src.p_over_rho_src = p->p_over_rho_src;
     f->src.r_floor = p->r_floor;
-    bool ok = upload(&f->cell_center, cell_center, 3 * (size_t)N, s) == cudaSuccess &&
-              upload(&f->cell_volume, cell_volume, (size_t)N, s) == cudaSuccess &&
-              upload(&f->cell_gran, cell_gran, 6 * (size_t)N, s) == cudaSuccess &&
+    f->perm = cperm;
+    bool ok = upload(&f->cell_center, cell_center.data(), 3 * (size_t)N, s) == cudaSuccess &&
+              upload(&f->cell_volume, cell_volume.data(), (size_t)N, s) == cudaSuccess &&
+              upload(&f->cell_gran, cell_gran.data(), 6 * (size_t)N, s) == cudaSuccess &&
               upload(&f->cell_flag, flag.data(), (size_t)N, s) == cudaSuccess &&
-              upload(&f->normal, gran_normal, 3 * (size_t)G, s) == cudaSuccess &&
-              upload(&f->square, gran_square, (size_t)G, s) == cudaSuccess &&
+              upload(&f->normal, gran_normal.data(), 3 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->square, gran_square.data(), (size_t)G, s) == cudaSuccess &&
               upload(&f->geo, geo.data(), 4 * (size_t)G, s) == cudaSuccess &&
-              upload(&f->nb, gran_neighbour, 2 * (size_t)G, s) == cudaSuccess &&
-              upload(&f->nbt, gran_neighbour_tvd, 2 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->nb, gran_neighbour.data(), 2 * (size_t)G, s) == cudaSuccess &&
+              upload(&f->nbt, gran_neighbour_tvd.data(), 2 * (size_t)G, s) == cudaSuccess &&
               upload(&f->type, type.data(), (size_t)G, s) == cudaSuccess &&
               cudaMalloc(&f->prim, sizeof(double) * 8 * (size_t)N) == cudaSuccess &&
               cudaMalloc(&f->flux, sizeof(double) * 8 * (size_t)G) == cudaSuccess &&
@@ -423,4 +499,8 @@ cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const doubl
     return cudaGetLastError();
 }
 
+}  // namespace sb
+
+namespace sb {
+const int32_t* fl_perm(const FaceListDev* f) { return f ? f->perm.data() : nullptr; }
 }  // namespace sb

@@ -318,6 +318,9 @@ int fl_create(FaceListDev** out, int64_t n_cell, int64_t n_gran, const double* c
               const double* gran_center, const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd,
               const int32_t* gran_type, const setb_fl_params* p, cudaStream_t s);
 void fl_destroy(FaceListDev* f);
+// Locality order of a face-list handle: device cell d is the caller's cell perm[d] (0-based);
+// null for a null handle.
+const int32_t* fl_perm(const FaceListDev* f);
 // One stage on the face list: primitive pass, face fluxes (+ dt candidate when want_dt), cell
 // update (kind 0: Euler / Heun stage 1, kind 1: Heun stage 2); a finalizing stage rolls the clock.
 cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const double* Ubase, double* Uout, int64_t vs,
