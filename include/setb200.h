@@ -222,6 +222,35 @@ SETB_API int32_t setb_init_facelist(setb_handle** h, int32_t n_cell, int32_t n_g
                                     const int32_t* gran_neighbour, const int32_t* gran_neighbour_tvd,
                                     const int32_t* gran_type, const setb_fl_params* params);
 
+/* ------------------------------------------------------------------ on-disk formats
+ * The grid/state stream file the reference's grid generator writes (SET_Gelios/source/
+ * Setka.cpp:1158-1567) and its FCMHD host reads (Set_Storage, Storage_module.f90:42-100):
+ * unformatted stream, no record markers, native byte order:
+ *   real(8) time_all, integer(4) N_cell, integer(4) N_gran, Cell_par(16,N), Cell_center(3,N),
+ *   Cell_Volume(N), integer(4) Cell_gran(6,N), Gran_normal(3,G), Gran_square(G), Gran_center(3,G),
+ *   integer(4) Gran_neighbour(2,G), integer(4) Gran_neighbour_TVD(2,G), real(8) 121.0,
+ *   integer(4) Gran_type(G), real(8) 122.0, Gran_POTOK(9,G), real(8) 123.0
+ * and the checkpoint of Save_Storage / Fill_data (Storage_module.f90:160-209):
+ *   real(8) time_all, Cell_par(16,N), real(8) 321.0
+ * A short file, a wrong sentinel, trailing bytes or counts that differ from the caller's give
+ * SETB_EIO (the reference printed the sentinel and went on). */
+SETB_API int32_t setb_fcmhd_read_header(const char* path, double* time_all, int32_t* n_cell, int32_t* n_gran);
+/* Reads the whole file into caller buffers sized for n_cell / n_gran (from the header);
+ * gran_potok (9*G doubles) may be NULL to skip the stored fluxes. */
+SETB_API int32_t setb_fcmhd_read(const char* path, int32_t n_cell, int32_t n_gran, double* time_all, double* cell_par,
+                                 double* cell_center, double* cell_volume, int32_t* cell_gran, double* gran_normal,
+                                 double* gran_square, double* gran_center, int32_t* gran_neighbour,
+                                 int32_t* gran_neighbour_tvd, int32_t* gran_type, double* gran_potok);
+/* Writes the file; gran_potok NULL writes zero fluxes, as the grid generator does. */
+SETB_API int32_t setb_fcmhd_write(const char* path, double time_all, int32_t n_cell, int32_t n_gran,
+                                  const double* cell_par, const double* cell_center, const double* cell_volume,
+                                  const int32_t* cell_gran, const double* gran_normal, const double* gran_square,
+                                  const double* gran_center, const int32_t* gran_neighbour,
+                                  const int32_t* gran_neighbour_tvd, const int32_t* gran_type, const double* gran_potok);
+/* Replaces Save_Storage / Fill_data (Storage_module.f90:160-209). */
+SETB_API int32_t setb_checkpoint_write(const char* path, double time_all, int32_t n_cell, const double* cell_par);
+SETB_API int32_t setb_checkpoint_read(const char* path, int32_t n_cell, double* time_all, double* cell_par);
+
 /* ------------------------------------------------------------------ batched solves
  * No counterpart in the reference (one grid per process, cuf_kernel.cuf:351-382).  A batch
  * advances many Cartesian solves of uneven size together: every step is two persistent launches

@@ -105,6 +105,13 @@ _SIGS = {
                                       _dp, _dp, C.POINTER(Diag), C.c_void_p]),
     "setb_init_facelist": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, _dp, _dp, _dp, _ip, _dp, _dp,
                                        _dp, _ip, _ip, _ip, C.c_void_p]),
+    "setb_fcmhd_read_header": (C.c_int32, [C.c_char_p, _dp, _ip, _ip]),
+    "setb_fcmhd_read": (C.c_int32, [C.c_char_p, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _ip, _dp, _dp, _dp, _ip,
+                                    _ip, _ip, _dp]),
+    "setb_fcmhd_write": (C.c_int32, [C.c_char_p, C.c_double, C.c_int32, C.c_int32, _dp, _dp, _dp, _ip, _dp, _dp,
+                                     _dp, _ip, _ip, _ip, _dp]),
+    "setb_checkpoint_write": (C.c_int32, [C.c_char_p, C.c_double, C.c_int32, _dp]),
+    "setb_checkpoint_read": (C.c_int32, [C.c_char_p, C.c_int32, _dp, _dp]),
     "setb_batch_create": (C.c_int32, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_int64]),
     "setb_batch_add": (C.c_int32, [C.c_void_p, C.POINTER(CartDesc), C.POINTER(LismIC), C.POINTER(StepOpts), _ip]),
     "setb_batch_remove": (C.c_int32, [C.c_void_p, C.c_int32]),

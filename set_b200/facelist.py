@@ -203,3 +203,57 @@ class FaceListSolver(Solver):
                                       i32(m.gran_type), C.byref(params))
         _check(rc, "setb_init_facelist")
         self.h = h
+
+
+# ---------------------------------------------------------------------------- on-disk formats
+def _i32p(a):
+    return a.ctypes.data_as(_ip)
+
+
+def read_fcmhd(path: str):
+    """The reference's grid/state stream file (Set_Storage, Storage_module.f90:42-100): returns
+    (time_all, cell_par [N,16], FaceList, gran_potok [G,9])."""
+    t = C.c_double()
+    n, g = C.c_int32(), C.c_int32()
+    bpath = str(path).encode()
+    _check(lib().setb_fcmhd_read_header(bpath, C.byref(t), C.byref(n), C.byref(g)), "setb_fcmhd_read_header")
+    N, G = n.value, g.value
+    cp = np.zeros((N, 16))
+    m = FaceList(cell_center=np.zeros((N, 3)), cell_volume=np.zeros(N), cell_gran=np.zeros((N, 6), np.int32),
+                 gran_normal=np.zeros((G, 3)), gran_square=np.zeros(G), gran_center=np.zeros((G, 3)),
+                 gran_neighbour=np.zeros((G, 2), np.int32), gran_neighbour_tvd=np.zeros((G, 2), np.int32),
+                 gran_type=np.zeros(G, np.int32))
+    potok = np.zeros((G, 9))
+    _check(lib().setb_fcmhd_read(bpath, N, G, C.byref(t), _p(cp), _p(m.cell_center), _p(m.cell_volume),
+                                 _i32p(m.cell_gran), _p(m.gran_normal), _p(m.gran_square), _p(m.gran_center),
+                                 _i32p(m.gran_neighbour), _i32p(m.gran_neighbour_tvd), _i32p(m.gran_type),
+                                 _p(potok)), "setb_fcmhd_read")
+    return t.value, cp, m, potok
+
+
+def write_fcmhd(path: str, time_all: float, cell_par: np.ndarray, m: FaceList, gran_potok: np.ndarray | None = None):
+    """Writes the grid/state stream file in the reference's format (zero fluxes when gran_potok
+    is None, as the grid generator writes them)."""
+    cp = np.ascontiguousarray(cell_par, dtype=np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    cg, nb, nbt, ty = i32(m.cell_gran), i32(m.gran_neighbour), i32(m.gran_neighbour_tvd), i32(m.gran_type)
+    pot = None if gran_potok is None else np.ascontiguousarray(gran_potok, dtype=np.float64)
+    _check(lib().setb_fcmhd_write(str(path).encode(), float(time_all), m.n_cell, m.n_gran, _p(cp), _p(m.cell_center),
+                                  _p(m.cell_volume), _i32p(cg), _p(m.gran_normal), _p(m.gran_square),
+                                  _p(m.gran_center), _i32p(nb), _i32p(nbt), _i32p(ty),
+                                  _p(pot) if pot is not None else None), "setb_fcmhd_write")
+
+
+def write_checkpoint(path: str, time_all: float, cell_par: np.ndarray):
+    """Save_Storage (Storage_module.f90:160-182): time, Cell_par(16,N), 321.0."""
+    cp = np.ascontiguousarray(cell_par, dtype=np.float64)
+    _check(lib().setb_checkpoint_write(str(path).encode(), float(time_all), cp.shape[0], _p(cp)),
+           "setb_checkpoint_write")
+
+
+def read_checkpoint(path: str, n_cell: int):
+    """Fill_data (Storage_module.f90:191-209): returns (time_all, cell_par [N,16])."""
+    t = C.c_double()
+    cp = np.zeros((n_cell, 16))
+    _check(lib().setb_checkpoint_read(str(path).encode(), int(n_cell), C.byref(t), _p(cp)), "setb_checkpoint_read")
+    return t.value, cp
