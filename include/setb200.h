@@ -213,6 +213,15 @@ typedef struct {
                                    0 = none                                                      */
     double cell_freeze_radius;  /* cells nearer the origin are not updated (reference: 0.05,
                                    cuf_solvers.cuf:611); 0 = none                                */
+    int32_t physics;            /* 0: conservative 3D ideal MHD of all 8 variables.
+                                   1: the reference's live cell update, 2D axisymmetric hydro
+                                   about the x axis (cuf_solvers.cuf:561-794): rr(2) = y is the
+                                   radius, geometric terms rho*v/y..., w = B = 0, charge exchange
+                                   with the two H-atom fluids of Cell_par columns 9..16
+                                   (Source_MK, cuf_kernel.cuf:215-288), the v clamp near the
+                                   axis (:783-785) and the Lax flux on near-axis faces
+                                   (cuf_solvers.cuf:293-295).  Cell centres need y > 0.          */
+    int32_t reserved;           /* must be 0                                                     */
 } setb_fl_params;
 
 /* Replaces Set_CUDA for the reference's grid (cuf_kernel.cuf:351-382). */

@@ -243,13 +243,20 @@ class OrcFaceList(C.Structure):
                 ("gran_type", C.POINTER(C.c_int32)),
                 ("r_src", C.c_double), ("rho_src", C.c_double), ("v_src", C.c_double),
                 ("p_over_rho_src", C.c_double), ("r_floor", C.c_double), ("dt_init", C.c_double),
-                ("face_skip_radius", C.c_double), ("cell_freeze_radius", C.c_double)]
+                ("face_skip_radius", C.c_double), ("cell_freeze_radius", C.c_double),
+                ("hatom", _dp), ("physics", C.c_int32), ("reserved", C.c_int32)]
 
 
-def facelist(mesh, params) -> OrcFaceList:
+def facelist(mesh, params, cell_par=None) -> OrcFaceList:
     """Oracle view of a face list (arrays in the reference's layouts, 1-based) and its
-    parameters (anything with the fields of setb_fl_params).  Keep `mesh` alive while used."""
+    parameters (anything with the fields of setb_fl_params); cell_par [N,16] supplies the H-atom
+    fluids (columns 9..16) of physics 1.  Keep `mesh` and the returned object's `_keep` alive."""
     m = OrcFaceList()
+    m.physics, m.reserved = int(getattr(params, "physics", 0)), 0
+    if cell_par is not None:
+        h = np.ascontiguousarray(np.asarray(cell_par, dtype=np.float64)[:, 8:16])
+        m.hatom = _p(h)
+        m._keep = h
     m.n_cell, m.n_gran = mesh.n_cell, mesh.n_gran
     i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
     m.cell_center, m.cell_volume, m.cell_gran = _p(mesh.cell_center), _p(mesh.cell_volume), i32(mesh.cell_gran)

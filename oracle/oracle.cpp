@@ -907,7 +907,44 @@ typedef struct {
     double dt_init;
     double face_skip_radius;    // faces whose first cell has |centre| < this are skipped
     double cell_freeze_radius;  // cells with |centre| < this are not updated
+    const double* hatom;        // physics 1: Cell_par columns 9..16 per cell ([N][8]), or null
+    int32_t physics, reserved;  // 0: 3D MHD conservative update; 1: the reference's axisymmetric
+                                // hydro update with charge exchange
 } orc_facelist;
+
+// SET_Fortran_Cuda_MHD/cuf_kernel.cuf:215-288, Source_MK: charge-exchange momentum (x, y) and
+// energy sources of the plasma against two H-atom fluids (rho, u, v, T in Cell_par columns
+// 9..12 and 13..16).  Default-real literals are single precision in the reference and enter as
+// their promoted values; 3.0/0.4326569 is a single-precision quotient.
+static void source_mk(const double* q, const double* h, double* out) {
+    const double pi = std::acos(-1.0);
+    const double rho = q[0], u = q[1], v = q[2], p = q[4];
+    const double small = (double)0.0000001f;
+    const double c_m = 64.0 / (9.0 * pi), c_u = 4.0 / pi;
+    const double c_s = (double)0.1307345665f;
+    const double c_n = (double)(3.0f / 0.4326569f);
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    for (int k = 0; k < 2; k++) {
+        double rH = h[4 * k], uH = h[4 * k + 1], vH = h[4 * k + 2];
+        double pH = 0.5 * h[4 * k + 3] * rH;
+        if (rH < small) {
+            rH = small;
+            pH = 0.0;
+        }
+        const double du = u - uH, dv = v - vH;
+        const double th = p / rho + 2.0 * pH / rH;
+        const double UM = std::sqrt((du * du + dv * dv) + c_m * th);
+        const double UH = std::sqrt((du * du + dv * dv) + c_u * th);
+        const double sg = (1.0 - c_s * std::log(UM)) * (1.0 - c_s * std::log(UM));
+        const double nu = ((rho * rH) * UM) * sg;
+        s1 = s1 + (c_n * nu) * (uH - u);
+        s2 = s2 + (c_n * nu) * (vH - v);
+        s3 = s3 + (c_n * nu) * ((((uH * uH + vH * vH) - u * u) - v * v) / 2.0 + (UH / UM) * (2.0 * pH / rH - p / rho));
+    }
+    out[0] = s1;
+    out[1] = s2;
+    out[2] = s3;
+}
 
 static double norm3(const double* x) { return std::sqrt((x[0] * x[0] + x[1] * x[1]) + x[2] * x[2]); }
 
@@ -984,7 +1021,10 @@ static double fl_face(const orc_facelist* m, const orc_opts* o, const double* P,
     if (q1[0] < 0.0 || q2[0] < 0.0) nrec++;      // :414-420
     double dsl, dsp, dsc, pot[8];
     const double wc = 0.0;
-    const int rc = chlld(o->n_state, n[0], n[1], n[2], wc, q1, q2, dsl, dsp, dsc, pot, o->n_disc);
+    int metod = o->n_state;
+    if (m->physics == 1 && gc[0] > (double)0.22f && gc[1] < (double)0.1f && std::fabs(n[0]) < (double)0.1f)
+        metod = 0;                                // :293-295, Lax flux on near-axis faces
+    const int rc = chlld(metod, n[0], n[1], n[2], wc, q1, q2, dsl, dsp, dsc, pot, o->n_disc);
     if (rc) {
         nwave++;
         for (int v = 0; v < 8; v++) pot[v] = 0.0;
@@ -1026,8 +1066,61 @@ static void fl_stage(const orc_facelist* m, const orc_opts* o, const double* Uin
             double un[8], qs[8];
             if (m->cell_freeze_radius > 0.0 && norm3(x) < m->cell_freeze_radius) {   // :611
                 for (int v = 0; v < 8; v++) un[v] = kind == 0 ? Uin[v * N + c] : Ubase[v * N + c];
-            } else if (source_prim(&sg, x, qs)) {
+            } else if (m->physics == 0 && source_prim(&sg, x, qs)) {
                 cons_from_prim(qs, un);
+            } else if (m->physics == 1) {
+                // cuf_solvers.cuf:561-794: the axisymmetric hydro update of the primitive state,
+                // restated with the reference's operation order; rr(2) = y
+                double pot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (int f = 0; f < 6; f++) {
+                    const int32_t j = m->cell_gran[6 * c + f];
+                    if (j == 0) continue;
+                    const double* Fj = Fl + 9 * (int64_t)(j - 1);
+                    const bool owner = m->gran_neighbour[2 * (int64_t)(j - 1)] == (int32_t)(c + 1);
+                    for (int v = 0; v < 8; v++) pot[v] = owner ? pot[v] + Fj[v] : pot[v] - Fj[v];
+                }
+                double q[8], q2[8], u8[8], source[3];
+                for (int v = 0; v < 8; v++) u8[v] = Uin[v * N + c];
+                prim_from_cons(u8, q);                               // qqq: the stage input
+                if (kind == 1) {
+                    for (int v = 0; v < 8; v++) u8[v] = Ubase[v * N + c];
+                    prim_from_cons(u8, q2);                          // qqq2: Cell_par
+                }
+                source_mk(q, m->hatom + 8 * c, source);
+                const double vol = m->cell_volume[c], y = x[1], t = dt;
+                const double nq = std::sqrt((q[1] * q[1] + q[2] * q[2]) + q[3] * q[3]);
+                const double e1 = q[4] / (ggg - 1.0) + 0.5 * q[0] * (nq * nq);
+                const double geo_e = (t * q[2]) * (ggg * q[4] / (ggg - 1) + q[0] * (q[1] * q[1] + q[2] * q[2]) * 0.5) / y;
+                double ro3, u3, v3, p3;
+                if (kind == 0) {
+                    ro3 = q[0] - t * (pot[0] / vol + q[0] * q[2] / y);
+                } else {
+                    ro3 = 0.5 * (q2[0] + q[0] - t * (pot[0] / vol + q[0] * q[2] / y));
+                }
+                if (ro3 <= 0.0) {                                    // :708-711 (STOP there)
+                    nneg++;
+                    if (local_first < 0) local_first = c;
+                    for (int v = 0; v < 8; v++) un[v] = Uin[v * N + c];
+                } else {
+                    if (kind == 0) {
+                        u3 = ((((q[0] * q[1] - t * (pot[1]) / vol) + t * source[0]) - ((t * q[0]) * q[1]) * q[2] / y)) / ro3;
+                        v3 = ((((q[0] * q[2] - t * (pot[2]) / vol) + t * source[1]) - ((t * q[0]) * q[2]) * q[2] / y)) / ro3;
+                        p3 = ((((e1 - t * (pot[4]) / vol) + t * source[2]) - geo_e) - 0.5 * ro3 * ((u3 * u3 + v3 * v3) + 0.0)) * (ggg - 1.0);
+                    } else {
+                        const double nq2 = std::sqrt((q2[1] * q2[1] + q2[2] * q2[2]) + q2[3] * q2[3]);
+                        const double e2 = q2[4] / (ggg - 1.0) + 0.5 * q2[0] * (nq2 * nq2);
+                        u3 = 0.5 * ((((q2[0] * q2[1] + q[0] * q[1]) - t * (pot[1]) / vol) + t * source[0]) - ((t * q[0]) * q[1]) * q[2] / y) / ro3;
+                        v3 = 0.5 * ((((q2[0] * q2[2] + q[0] * q[2]) - t * (pot[2]) / vol) + t * source[1]) - ((t * q[0]) * q[2]) * q[2] / y) / ro3;
+                        p3 = (0.5 * ((((e2 + e1) - t * (pot[4]) / vol) + t * source[2]) - geo_e) - 0.5 * ro3 * ((u3 * u3 + v3 * v3) + 0.0)) * (ggg - 1.0);
+                    }
+                    if (p3 <= 0.0) {                                 // :777-779
+                        nfloor++;
+                        p3 = p_floor;
+                    }
+                    if (x[0] > (double)0.28f && x[1] < (double)0.07f && v3 < 0.0) v3 = (double)0.01f;   // :783-785
+                    const double qn[8] = {ro3, u3, v3, 0.0, p3, 0.0, 0.0, 0.0};
+                    cons_from_prim(qn, un);
+                }
             } else {
                 double pot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 for (int f = 0; f < 6; f++) {                                         // :691-703

@@ -248,6 +248,8 @@ int upload_cellpar(setb_handle* h, const double* cell_par) {
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
     double* stage = h->buf[1 - h->cur];
     if (const int32_t* perm = fl_perm(h->fl)) {
+        const int rc = fl_set_hatom(h->fl, cell_par, h->stream);
+        if (rc) return rc;
         std::vector<double> tmp(8 * N);
         for (size_t d = 0; d < N; d++) std::memcpy(&tmp[8 * d], cell_par + 16 * (size_t)perm[d], 8 * sizeof(double));
         SB_TRY(cudaMemcpyAsync(stage, tmp.data(), sizeof(double) * 8 * N, cudaMemcpyHostToDevice, h->stream));
@@ -396,7 +398,11 @@ int32_t setb_init_facelist(setb_handle** out, int32_t n_cell, int32_t n_gran, co
                            const setb_fl_params* params) {
     if (!out || !cell_par || !params || n_cell < 1 || n_gran < 1) return SETB_EINVAL;
     *out = nullptr;
-    if (!(params->dt_init > 0.0)) return SETB_EINVAL;
+    if (!(params->dt_init > 0.0) || params->physics < 0 || params->physics > 1 || params->reserved != 0)
+        return SETB_EINVAL;
+    if (params->physics == 1)   // the axisymmetric update divides by the radius y
+        for (int32_t c = 0; c < n_cell; c++)
+            if (!(cell_center[3 * (size_t)c + 1] > 0.0)) return SETB_EINVAL;
     int rc = fl_validate(n_cell, n_gran, cell_center, cell_volume, cell_gran, gran_normal, gran_square, gran_center,
                          gran_neighbour, gran_neighbour_tvd, gran_type);
     if (rc) return rc;

@@ -44,11 +44,14 @@ struct FaceListDev {
     double* geo = nullptr;           // [G][4]: dist = |c_face - c_s1|, df2, dff1, dff2
     int32_t* nb = nullptr;           // [G][2], 1-based, -1 = none
     int32_t* nbt = nullptr;          // [G][2], 1-based, -1 = none
-    int32_t* type = nullptr;         // [G]: 0 = skipped, else the reference's face type 1..5
+    int32_t* type = nullptr;         // [G]: 0 = skipped, else the reference's face type 1..5,
+                                     // plus kLaxFace on the near-axis faces of physics 1
     // work
     double* prim = nullptr;          // [N][8] primitive state of the stage input
     double* flux = nullptr;          // [G][8] face flux * area (persistent)
     GridGeom src{};                  // source-sphere parameters (r_src 0 = none)
+    int physics = 0;                 // 0: 3D MHD; 1: the reference's axisymmetric hydro update
+    double* hatom = nullptr;         // physics 1: [N][8] H-atom fluids (Cell_par columns 9..16)
     // locality order: device cell d holds the caller's cell perm[d] (both 0-based)
     std::vector<int32_t> perm;
 };
@@ -56,6 +59,7 @@ struct FaceListDev {
 namespace {
 
 constexpr int kFaceThreads = 128, kCellThreads = 256, kPrimThreads = 256;
+constexpr int kLaxFace = 8;   // face-type bit: the reference's Lax flux on near-axis faces
 
 double norm3(const double* x) {
     return std::sqrt((x[0] * x[0] + x[1] * x[1]) + x[2] * x[2]);
@@ -98,6 +102,109 @@ __device__ __forceinline__ void load_prim(const double* P, int64_t c, double* q)
     }
 }
 
+// Source_MK (SET_Fortran_Cuda_MHD/cuf_kernel.cuf:215-288): charge-exchange momentum (x, y) and
+// energy sources against two H-atom fluids (rho, u, v, T per fluid in h[0..3], h[4..7]).  The
+// reference's default-real literals enter as their single-precision values.
+__device__ __forceinline__ void source_mk(const double* q, const double* h, double* out) {
+    const double pi = 3.141592653589793;
+    const double rho = q[0], u = q[1], v = q[2], p = q[4];
+    const double small = (double)0.0000001f;
+    const double c_m = __ddiv_rn(64.0, dmul(9.0, pi)), c_u = __ddiv_rn(4.0, pi);
+    const double c_s = (double)0.1307345665f;
+    const double c_n = (double)(3.0f / 0.4326569f);
+    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        double rH = h[4 * k], uH = h[4 * k + 1], vH = h[4 * k + 2];
+        double pH = dmul(dmul(0.5, h[4 * k + 3]), rH);
+        if (rH < small) {
+            rH = small;
+            pH = 0.0;
+        }
+        const double du = dsub(u, uH), dv = dsub(v, vH);
+        const double th = dadd(__ddiv_rn(p, rho), __ddiv_rn(dmul(2.0, pH), rH));
+        const double d2 = dadd(dmul(du, du), dmul(dv, dv));
+        const double UM = sqrt(dadd(d2, dmul(c_m, th)));
+        const double UH = sqrt(dadd(d2, dmul(c_u, th)));
+        const double lg = dsub(1.0, dmul(c_s, log(UM)));
+        const double nu = dmul(dmul(dmul(rho, rH), UM), dmul(lg, lg));
+        const double cn = dmul(c_n, nu);
+        s1 = dadd(s1, dmul(cn, dsub(uH, u)));
+        s2 = dadd(s2, dmul(cn, dsub(vH, v)));
+        const double ke = __ddiv_rn(dsub(dsub(dadd(dmul(uH, uH), dmul(vH, vH)), dmul(u, u)), dmul(v, v)), 2.0);
+        s3 = dadd(s3, dmul(cn, dadd(ke, dmul(__ddiv_rn(UH, UM), dsub(__ddiv_rn(dmul(2.0, pH), rH), __ddiv_rn(p, rho))))));
+    }
+    out[0] = s1;
+    out[1] = s2;
+    out[2] = s3;
+}
+
+// The reference's live cell update (cuf_solvers.cuf:561-794): 2D axisymmetric hydro about the x
+// axis with radius rr(2) = y, w = B = 0, charge exchange, p floor and the near-axis v clamp, in
+// the reference's operation order on the primitive state.  Writes the conserved result to un;
+// returns 1 for a non-positive density (un = the stage input), 2 when the p floor applied.
+template <int KIND>
+__device__ __forceinline__ int axisym_update(const double* Uin, const double* Ubase, int64_t vs, int64_t c,
+                                             const double* pot, double vol, double x, double y, const double* h,
+                                             double t, double* un) {
+    const double g = kGamma, gm1 = dsub(kGamma, 1.0);
+    double u8[8], q[8], q2[8], ke, me, source[3];
+#pragma unroll
+    for (int v = 0; v < 8; v++) u8[v] = Uin[v * vs + c];
+    prim_from_cons_exact(u8, q);
+    if (KIND == 1) {
+        double b8[8];
+#pragma unroll
+        for (int v = 0; v < 8; v++) b8[v] = Ubase[v * vs + c];
+        prim_from_cons_exact(b8, q2);
+    }
+    (void)ke;
+    (void)me;
+    source_mk(q, h, source);
+    const double nq = sqrt(dadd(dadd(dmul(q[1], q[1]), dmul(q[2], q[2])), dmul(q[3], q[3])));
+    const double e1 = dadd(__ddiv_rn(q[4], gm1), dmul(dmul(0.5, q[0]), dmul(nq, nq)));
+    const double X = dadd(__ddiv_rn(dmul(g, q[4]), gm1), dmul(dmul(q[0], dadd(dmul(q[1], q[1]), dmul(q[2], q[2]))), 0.5));
+    const double geo_e = __ddiv_rn(dmul(dmul(t, q[2]), X), y);
+    const double div0 = dadd(__ddiv_rn(pot[0], vol), __ddiv_rn(dmul(q[0], q[2]), y));
+    double ro3;
+    if (KIND == 0) ro3 = dsub(q[0], dmul(t, div0));
+    else ro3 = dmul(0.5, dsub(dadd(q2[0], q[0]), dmul(t, div0)));
+    if (!(ro3 > 0.0)) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) un[v] = u8[v];
+        return 1;
+    }
+    const double g1 = __ddiv_rn(dmul(t, pot[1]), vol), g2 = __ddiv_rn(dmul(t, pot[2]), vol);
+    const double g4 = __ddiv_rn(dmul(t, pot[4]), vol);
+    const double a1 = __ddiv_rn(dmul(dmul(dmul(t, q[0]), q[1]), q[2]), y);
+    const double a2 = __ddiv_rn(dmul(dmul(dmul(t, q[0]), q[2]), q[2]), y);
+    double u3, v3, p3;
+    if (KIND == 0) {
+        u3 = __ddiv_rn(dsub(dadd(dsub(dmul(q[0], q[1]), g1), dmul(t, source[0])), a1), ro3);
+        v3 = __ddiv_rn(dsub(dadd(dsub(dmul(q[0], q[2]), g2), dmul(t, source[1])), a2), ro3);
+        p3 = dmul(dsub(dsub(dadd(dsub(e1, g4), dmul(t, source[2])), geo_e),
+                       dmul(dmul(0.5, ro3), dadd(dadd(dmul(u3, u3), dmul(v3, v3)), 0.0))),
+                  gm1);
+    } else {
+        const double nq2 = sqrt(dadd(dadd(dmul(q2[1], q2[1]), dmul(q2[2], q2[2])), dmul(q2[3], q2[3])));
+        const double e2 = dadd(__ddiv_rn(q2[4], gm1), dmul(dmul(0.5, q2[0]), dmul(nq2, nq2)));
+        u3 = __ddiv_rn(dmul(0.5, dsub(dadd(dsub(dadd(dmul(q2[0], q2[1]), dmul(q[0], q[1])), g1), dmul(t, source[0])), a1)), ro3);
+        v3 = __ddiv_rn(dmul(0.5, dsub(dadd(dsub(dadd(dmul(q2[0], q2[2]), dmul(q[0], q[2])), g2), dmul(t, source[1])), a2)), ro3);
+        p3 = dmul(dsub(dmul(0.5, dsub(dadd(dsub(dadd(e2, e1), g4), dmul(t, source[2])), geo_e)),
+                       dmul(dmul(0.5, ro3), dadd(dadd(dmul(u3, u3), dmul(v3, v3)), 0.0))),
+                  gm1);
+    }
+    int rc = 0;
+    if (p3 <= 0.0) {
+        p3 = kPFloor;
+        rc = 2;
+    }
+    if (x > (double)0.28f && y < (double)0.07f && v3 < 0.0) v3 = (double)0.01f;
+    const double qn[8] = {ro3, u3, v3, 0.0, p3, 0.0, 0.0, 0.0};
+    cons_from_prim_exact(qn, un);
+    return rc;
+}
+
 // One face per thread, cuf_solvers.cuf:243-440 (face speed 0).
 template <int NSTATE, int ORDER, bool WANT_DT>
 __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceListDev m, double cfl, int n_disc,
@@ -109,7 +216,8 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
     const int64_t gr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     double cand = kDtReset;
     unsigned n_recon = 0, n_wave = 0;
-    const int type = gr < m.n_gran ? m.type[gr] : 0;
+    const int tword = gr < m.n_gran ? m.type[gr] : 0;
+    const int type = tword & 7;
     if (type != 0) {
         const int64_t s1 = m.nb[2 * gr] - 1;
         const int32_t s2r = m.nb[2 * gr + 1];
@@ -163,7 +271,8 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
         if (q1[0] < 0.0 || q2[0] < 0.0) n_recon++;
         double qqq[8], sp[3];
         int32_t fl = 0;
-        chlld_general<double, NSTATE>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);
+        if (tword & kLaxFace) chlld_general<double, 0>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);   // :293-295
+        else chlld_general<double, NSTATE>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);
         if (fl & kFlagWave) {
             n_wave++;
 #pragma unroll
@@ -216,9 +325,33 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
         if (m.cell_flag[c] & 1) {
 #pragma unroll
             for (int v = 0; v < 8; v++) un[v] = KIND == 0 ? Uin[v * vs + c] : Ubase[v * vs + c];
-        } else if (m.src.r_src > 0.0 && r2 < dmul(m.src.r_src, m.src.r_src)) {
+        } else if (m.physics == 0 && m.src.r_src > 0.0 && r2 < dmul(m.src.r_src, m.src.r_src)) {
             source_state(m.src, x, y, z, r2, qs);
             cons_from_prim_exact(qs, un);
+        } else if (m.physics == 1) {
+            double pot[8];
+#pragma unroll
+            for (int v = 0; v < 8; v++) pot[v] = 0.0;
+            for (int f = 0; f < 6; f++) {
+                const int32_t j = m.cell_gran[6 * c + f];
+                if (j == 0) continue;
+                const int64_t jf = (int64_t)j - 1;
+                const bool owner = m.nb[2 * jf] == (int32_t)(c + 1);
+                const double2* f2 = reinterpret_cast<const double2*>(m.flux + 8 * jf);
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    const double2 d = f2[v];
+                    pot[2 * v] = owner ? pot[2 * v] + d.x : pot[2 * v] - d.x;
+                    pot[2 * v + 1] = owner ? pot[2 * v + 1] + d.y : pot[2 * v + 1] - d.y;
+                }
+            }
+            const int rc = axisym_update<KIND>(Uin, Ubase, vs, c, pot, m.cell_volume[c], x, y, m.hatom + 8 * c, dt, un);
+            if (rc == 1) {
+                atomicAdd(&cnt[0], 1ull);
+                atomicMin(&st->first_bad, (unsigned long long)c);
+            } else if (rc == 2) {
+                atomicAdd(&cnt[1], 1ull);
+            }
         } else {
             double pot[8];
 #pragma unroll
@@ -301,8 +434,8 @@ void launch_face_n(const FaceListDev& m, int order, bool want_dt, double cfl, in
 // ------------------------------------------------------------------------------ host side
 void fl_destroy(FaceListDev* f) {
     if (!f) return;
-    void* ptrs[] = {f->cell_center, f->cell_volume, f->cell_gran, f->cell_flag, f->normal, f->square,
-                    f->geo,         f->nb,          f->nbt,       f->type,      f->prim,   f->flux};
+    void* ptrs[] = {f->cell_center, f->cell_volume, f->cell_gran, f->cell_flag, f->normal, f->square, f->geo,
+                    f->nb,          f->nbt,         f->type,      f->prim,      f->flux,   f->hatom};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete f;
@@ -443,6 +576,10 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
         }
         // the reference skips faces whose first cell lies inside its frozen core (:284)
         type[g] = (p->face_skip_radius > 0.0 && norm3(c1) < p->face_skip_radius) ? 0 : t;
+        // physics 1: the reference's Lax flux on faces near the axis (cuf_solvers.cuf:293-295)
+        if (type[g] && p->physics == 1 && gc[0] > (double)0.22f && gc[1] < (double)0.1f &&
+            std::fabs(gran_normal[3 * g]) < (double)0.1f)
+            type[g] |= kLaxFace;
     }
     std::vector<unsigned char> flag((size_t)N);
     for (int64_t c = 0; c < N; c++)
@@ -458,6 +595,7 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
     f->src.p_over_rho_src = p->p_over_rho_src;
     f->src.r_floor = p->r_floor;
     f->perm = cperm;
+    f->physics = p->physics;
     bool ok = upload(&f->cell_center, cell_center.data(), 3 * (size_t)N, s) == cudaSuccess &&
               upload(&f->cell_volume, cell_volume.data(), (size_t)N, s) == cudaSuccess &&
               upload(&f->cell_gran, cell_gran.data(), 6 * (size_t)N, s) == cudaSuccess &&
@@ -470,6 +608,7 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
               upload(&f->type, type.data(), (size_t)G, s) == cudaSuccess &&
               cudaMalloc(&f->prim, sizeof(double) * 8 * (size_t)N) == cudaSuccess &&
               cudaMalloc(&f->flux, sizeof(double) * 8 * (size_t)G) == cudaSuccess &&
+              (p->physics != 1 || cudaMalloc(&f->hatom, sizeof(double) * 8 * (size_t)N) == cudaSuccess) &&
               cudaMemsetAsync(f->flux, 0, sizeof(double) * 8 * (size_t)G, s) == cudaSuccess &&
               cudaStreamSynchronize(s) == cudaSuccess;   // host vectors are released on return
     if (!ok) {
@@ -503,4 +642,18 @@ cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const doubl
 
 namespace sb {
 const int32_t* fl_perm(const FaceListDev* f) { return f ? f->perm.data() : nullptr; }
+}  // namespace sb
+
+namespace sb {
+// Uploads the H-atom fluids (Cell_par columns 9..16, caller numbering) of a physics-1 face list.
+int fl_set_hatom(FaceListDev* f, const double* cell_par, cudaStream_t s) {
+    if (!f || !f->hatom) return SETB_OK;
+    const size_t N = (size_t)f->n_cell;
+    std::vector<double> tmp(8 * N);
+    for (size_t d = 0; d < N; d++) std::memcpy(&tmp[8 * d], cell_par + 16 * (size_t)f->perm[d] + 8, 8 * sizeof(double));
+    if (cudaMemcpyAsync(f->hatom, tmp.data(), sizeof(double) * 8 * N, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return SETB_ECUDA;
+    return SETB_OK;
+}
 }  // namespace sb

@@ -321,6 +321,8 @@ void fl_destroy(FaceListDev* f);
 // Locality order of a face-list handle: device cell d is the caller's cell perm[d] (0-based);
 // null for a null handle.
 const int32_t* fl_perm(const FaceListDev* f);
+// Uploads the H-atom fluids (Cell_par columns 9..16) of a face list with physics 1; no-op else.
+int fl_set_hatom(FaceListDev* f, const double* cell_par, cudaStream_t s);
 // One stage on the face list: primitive pass, face fluxes (+ dt candidate when want_dt), cell
 // update (kind 0: Euler / Heun stage 1, kind 1: Heun stage 2); a finalizing stage rolls the clock.
 cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const double* Ubase, double* Uout, int64_t vs,

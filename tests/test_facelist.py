@@ -116,3 +116,29 @@ def test_init_facelist_validates_on_the_host():
     with pytest.raises(S.SetbError) as e:
         FL.FaceListSolver(bad, cp, params)
     assert e.value.code == 1
+
+
+def test_axisymmetric_physics_needs_positive_radius():
+    m = FL.box_facelist((4, 3, 2), lo=(-1.0, -0.5, -0.1), hi=(1.0, 0.5, 0.1), seed=1)
+    cp = FL.lism_cellpar(m)
+    with pytest.raises(S.SetbError) as e:
+        FL.FaceListSolver(m, cp, FL.fl_params(physics=1))
+    assert e.value.code == 1
+    with pytest.raises(S.SetbError) as e:
+        FL.FaceListSolver(m, cp, FL.fl_params(physics=2))
+    assert e.value.code == 1
+
+
+def test_oracle_source_mk_moves_plasma_towards_the_atoms():
+    """Charge exchange in the oracle's axisymmetric update: with fast H atoms along +x and the
+    plasma at rest, the plasma's x momentum grows (Source_MK, cuf_kernel.cuf:215-288)."""
+    m = FL.box_facelist((6, 5, 1), lo=(-1.0, 0.1, -0.02), hi=(1.0, 1.0, 0.02), seed=1,
+                        sides={"x-": 2, "x+": 2, "y-": 2, "y+": 2, "z-": 2, "z+": 2})
+    params = FL.fl_params(r_src=0.0, dt_init=1e-3, physics=1)
+    cp = FL.lism_cellpar(m, lism=np.array([1.0, 0, 0, 0, 1.0, 0, 0, 0]), pert_amp=0.0)
+    cp[:, 8:12] = [0.2, 3.0, 0.0, 1.0]
+    cp[:, 12:16] = [0.0, 0.0, 0.0, 1.0]
+    om = O.facelist(m, params, cell_par=cp)
+    U = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1).copy()
+    O.fl_run(om, O.make_opts(2, 1, 1, 0.4), U, 1)
+    assert (U[1] > 0).all()

@@ -97,3 +97,44 @@ def test_grid_file_drives_the_solver(tmp_path):
     Ua, ta, _ = gpu_run(m, params, cp, o, 8)
     Ub, tb, _ = gpu_run(m2, params, cp2, o, 8)
     assert t0 == 0.0 and np.array_equal(Ua, Ub) and ta == tb
+
+
+def axisym_case(seed=0, n=(24, 16, 1)):
+    """A thin box about the x axis (y >= 0 is the radius; the y = 0 side is the axis, type 5),
+    z faces are walls; plasma without field, two H-atom fluids in Cell_par columns 9..16."""
+    sides = {"x-": 4, "x+": 4, "y-": 5, "y+": 4, "z-": 2, "z+": 2}
+    m = FL.box_facelist(n, lo=(-1.0, 0.0, -0.02), hi=(1.0, 1.0, 0.02), stretch=0.3, sides=sides,
+                        permute_seed=seed + 1, seed=seed)
+    params = FL.fl_params(r_src=0.0, dt_init=1e-4, face_skip_radius=0.02, cell_freeze_radius=0.05, physics=1)
+    rng = np.random.default_rng(seed)
+    cp = FL.lism_cellpar(m, lism=S.lism_prim(bmag=0.0), seed=seed + 2, pert_amp=0.05)
+    N = m.n_cell
+    cp[:, 8] = rng.uniform(0.05, 0.2, N)       # rho_H3
+    cp[:, 9] = rng.uniform(-2.6, -2.2, N)      # u_H3
+    cp[:, 10] = rng.uniform(-0.1, 0.1, N)      # v_H3
+    cp[:, 11] = rng.uniform(0.5, 1.5, N)       # T_H3
+    cp[:, 12] = rng.uniform(0.01, 0.1, N)      # rho_H4
+    cp[:, 13] = rng.uniform(-2.0, -1.0, N)
+    cp[:, 14] = rng.uniform(-0.3, 0.3, N)
+    cp[:, 15] = rng.uniform(1.0, 3.0, N)
+    cp[:5, 12] = 0.0                            # below the reference's density floor
+    return m, params, cp
+
+
+@pytest.mark.parametrize("scheme", [2, 1])
+def test_axisymmetric_charge_exchange_matches_oracle(scheme):
+    m, params, cp = axisym_case(scheme)
+    opts_o = O.make_opts(2, 2, scheme, 0.4)
+    opts_g = S.step_opts(n_state=2, order=2, scheme=scheme, cfl=0.4)
+    om = O.facelist(m, params, cell_par=cp)
+    for steps, tol in ((1, 1e-12), (20, 1e-10)):
+        Uo = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1).copy()
+        cko, dgo, _ = O.fl_run(om, opts_o, Uo, steps)
+        Ug, tg, dg = gpu_run(m, params, cp, opts_g, steps)
+        assert np.isfinite(Ug).all()
+        l1 = np.abs(Ug - Uo).sum(1) / (np.abs(Uo).sum(1) + 1e-300)
+        assert l1.max() <= tol, (steps, l1)
+        assert abs(tg - cko.time_all) <= 1e-12 * cko.time_all
+        assert dg.n_negdens == dgo.n_negdens == 0
+    # the axisymmetric update keeps w and B at zero; charge exchange moves momentum
+    assert np.abs(Ug[3]).max() == 0.0 and np.abs(Ug[5:]).max() == 0.0
