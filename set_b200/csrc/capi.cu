@@ -97,10 +97,14 @@ GridGeom make_geom(const setb_cart_desc* d) {
     return g;
 }
 
+// The two tile heights a handle keeps tensor maps for, and which one a launch uses.
+constexpr int kShapeTy[2] = {tile_shape(0, 0).ty, tile_shape(1, 1).ty};
+int shape_index(int precision, int kind) { return tile_shape(precision, kind).ty == kShapeTy[0] ? 0 : 1; }
+
 // z extent of one CTA's march: balances wave quantisation against the per-chunk prologue
 // (4 plane loads + 1 z face, costed as ~1.5 plane iterations).
-int choose_lz(const GridGeom& g, int sm_count, int precision) {
-    const TileShape ts = tile_shape(precision);
+int choose_lz(const GridGeom& g, int sm_count, int precision, int kind) {
+    const TileShape ts = tile_shape(precision, kind);
     const long long cols = (long long)((g.nx + kTileX - 1) / kTileX) * ((g.ny + ts.ty - 1) / ts.ty);
     const long long slots = (long long)sm_count * std::max(ts.ctas_per_sm, 1);
     double best = 1e300;
@@ -194,8 +198,8 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
         return SETB_ECUDA;
     }
     h->sm_count = prop.multiProcessorCount;
-    h->ctas_per_sm = tile_shape(0).ctas_per_sm;
-    h->g.lz = choose_lz(h->g, h->sm_count, 0);
+    h->ctas_per_sm = tile_shape(0, 0).ctas_per_sm;
+    h->g.lz = choose_lz(h->g, h->sm_count, 0, 0);
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
         return SETB_ECUDA;
@@ -218,7 +222,7 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
         for (int shape = 0; shape < 2; shape++) {
             h->tma_ok[shape] = true;
             for (int b = 0; b < 2; b++)
-                if (encode_state_tmap(h->g, h->buf[b], shape == 0 ? 0 : 1, &tm[2 * b + shape]) != SETB_OK)
+                if (encode_state_tmap(h->g, h->buf[b], kShapeTy[shape], &tm[2 * b + shape]) != SETB_OK)
                     h->tma_ok[shape] = false;
         }
         if (cudaMalloc(&h->tmap, sizeof(tm)) != cudaSuccess ||
@@ -490,7 +494,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     StageArgs a{};
     a.g = h->g;
     const int P = o->precision;
-    a.g.lz = choose_lz(h->g, h->sm_count, P);
+    const int lz0 = choose_lz(h->g, h->sm_count, P, 0), lz1 = choose_lz(h->g, h->sm_count, P, 1);
     float* comp = nullptr;
     if (P != 0) {
         if (!h->comp) {
@@ -512,14 +516,15 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     a.st = h->st;
     a.cfl = o->cfl;
     a.n_disc = o->n_disc;
-    const int shape = P == 1 ? 1 : 0;
+    const int shape0 = shape_index(P, 0), shape1 = shape_index(P, 1);
     if (ev) SB_TRY(cudaEventRecord(ev[0], h->stream));
     for (int s = 0; s < nsteps; s++) {
         double* U = h->buf[h->cur];
         double* W = h->buf[1 - h->cur];
-        const CUtensorMap* tmU = h->tma_ok[shape] ? h->tmap + 2 * h->cur + shape : nullptr;
-        const CUtensorMap* tmW = h->tma_ok[shape] ? h->tmap + 2 * (1 - h->cur) + shape : nullptr;
+        const CUtensorMap* tmU = h->tma_ok[shape0] ? h->tmap + 2 * h->cur + shape0 : nullptr;
+        const CUtensorMap* tmW = h->tma_ok[shape1] ? h->tmap + 2 * (1 - h->cur) + shape1 : nullptr;
         if (o->scheme == 2) {
+            a.g.lz = lz0;
             a.Uin = U;
             a.tm_in = tmU;
             a.Ubase = nullptr;
@@ -528,6 +533,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
             a.comp = nullptr;
             SB_TRY(launch_stage(a, P, o->n_state, o->order, 0, true, h->stream));
             if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 1], h->stream));
+            a.g.lz = lz1;
             a.Uin = W;
             a.tm_in = tmW;
             a.Ubase = U;
@@ -537,6 +543,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
             SB_TRY(launch_stage(a, P, o->n_state, o->order, 1, false, h->stream));
             if (ev) SB_TRY(cudaEventRecord(ev[2 * s + 2], h->stream));
         } else {
+            a.g.lz = lz0;
             a.Uin = U;
             a.tm_in = tmU;
             a.Ubase = nullptr;

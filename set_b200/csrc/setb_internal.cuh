@@ -13,15 +13,18 @@ namespace sb {
 // 789-794); here the last CTA of each step's final kernel rolls the clock on the device, so a
 // run of steps needs no host round trip.
 // Column tile of the stage kernels: kTileX x ty cells marched along z by `threads` threads,
-// `ctas_per_sm` resident per SM; per form (precision 0 plain FP64, 1 mixed, 2 delta).  The
-// plain and delta forms fit FP64 HLLD in 168 registers (384 threads, 12 warps per SM); the mixed
-// form runs two 256-thread CTAs of at most 128 registers.
+// `ctas_per_sm` resident per SM; per form (precision 0 plain FP64, 1 mixed, 2 delta) and launch
+// (kind 0: Euler step / Heun stage 1; kind 1: Heun stage 2 and every batch launch).  The plain
+// and delta forms fit FP64 HLLD in 168 registers (384 threads, 12 warps per SM).  The mixed
+// form's first stage runs that shape too; its second stage, which also streams the FP32
+// compensation, runs two 256-thread CTAs of at most 128 registers, so one CTA's update overlaps
+// the other's faces.
 constexpr int kTileX = 32;
 struct TileShape {
     int ty, threads, ctas_per_sm;
 };
-SB_HD constexpr TileShape tile_shape(int precision) {
-    return precision == 1 ? TileShape{7, 256, 2} : TileShape{11, 384, 1};
+SB_HD constexpr TileShape tile_shape(int precision, int kind) {
+    return (precision == 1 && kind == 1) ? TileShape{7, 256, 2} : TileShape{11, 384, 1};
 }
 
 struct DevClock {
@@ -304,9 +307,9 @@ inline void set_device_strides(GridGeom& g) {
 }
 
 // Encodes the 4-D tensor map (x, y, z, variable) of the FP64 SoA state at `base` with geometry
-// g, box (kTileX + 4, tile_shape(precision).ty + 4, 1, 8): one plane of a column tile with its
-// 2-cell halo.  Returns a SETB_* status.
-int encode_state_tmap(const GridGeom& g, const double* base, int precision, CUtensorMap* out);
+// g, box (kTileX + 4, ty + 4, 1, 8): one plane of a column tile of ty rows with its 2-cell halo.
+// Returns a SETB_* status.
+int encode_state_tmap(const GridGeom& g, const double* base, int ty, CUtensorMap* out);
 
 // ---------------------------------------------------------------- face-list grids (facelist.cu)
 struct FaceListDev;
@@ -334,7 +337,7 @@ cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int ki
                               cudaStream_t s);
 cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
                          cudaStream_t s);
-int stage_smem_bytes(int precision);
+int stage_smem_bytes(int precision, int kind);
 cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
                                cudaStream_t s);
 cudaError_t prepare_batch_kernels(int precision);

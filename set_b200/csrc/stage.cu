@@ -35,9 +35,9 @@ namespace {
 // 3 TY + 2 warp jobs of a plane's faces (see run_tile) take three rounds of the CTA's warps
 // (32 x 7 cells: 23 jobs over 8 warps; 32 x 11: 35 jobs over 12 warps).  Threads 0..NC-1 own
 // one cell each in the update.
-template <int P> struct Tile {
-    static constexpr int TX = kTileX, TY = tile_shape(P).ty, NT = tile_shape(P).threads;
-    static constexpr int MINB = tile_shape(P).ctas_per_sm;
+template <int P, int SK> struct Tile {   // SK: the launch kind of tile_shape
+    static constexpr int TX = kTileX, TY = tile_shape(P, SK).ty, NT = tile_shape(P, SK).threads;
+    static constexpr int MINB = tile_shape(P, SK).ctas_per_sm;
     static constexpr int NC = TX * TY;
     static constexpr int HX = TX + 4, HY = TY + 4, PLANE = HX * HY;
     static constexpr int NXF = (TX + 1) * TY;        // x faces
@@ -70,9 +70,9 @@ __device__ __forceinline__ void fetch_prim64(const StageArgs& A, int i, int j, i
 }
 
 // Loads plane kk (with halo) of the tile starting at (i0, j0) as primitives into `dst`.
-template <int P, typename RT>
+template <int P, int SK, typename RT>
 __device__ __forceinline__ void load_plane(const StageArgs& A, RT* dst, int i0, int j0, int kk) {
-    constexpr int HX = Tile<P>::HX, PLANE = Tile<P>::PLANE, NT = Tile<P>::NT;
+    constexpr int HX = Tile<P, SK>::HX, PLANE = Tile<P, SK>::PLANE, NT = Tile<P, SK>::NT;
     for (int c = threadIdx.x; c < PLANE; c += NT) {
         const int cx = c % HX, cy = c / HX;
         double q[8];
@@ -128,9 +128,9 @@ __device__ __forceinline__ void tma_plane(void* dst, const CUtensorMap* tm, int 
 
 // Primitive plane with the boundary rules from a staged box (conserved, [v][y][x] with row HX):
 // inflow beyond x = hi, zero-gradient (clamped index, always inside the box) elsewhere.
-template <int P, typename RT>
+template <int P, int SK, typename RT>
 __device__ __forceinline__ void convert_plane(const StageArgs& A, const double* stg, RT* dst, int i0, int j0) {
-    constexpr int HX = Tile<P>::HX, PLANE = Tile<P>::PLANE, NT = Tile<P>::NT;
+    constexpr int HX = Tile<P, SK>::HX, PLANE = Tile<P, SK>::PLANE, NT = Tile<P, SK>::NT;
     const GridGeom& g = A.g;
     for (int c = threadIdx.x; c < PLANE; c += NT) {
         const int cx = c % HX, cy = c / HX;
@@ -236,13 +236,13 @@ __device__ __noinline__ int face_fp64_states(const double* q1, const double* q2,
     return riemann<double, NSTATE, false, false>(q1, q2, 0.0, n_disc, F, *sl, *sr, SM);
 }
 
-template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
+template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT, int SK>
 __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int bz, unsigned total_tiles,
                                          unsigned long long* bar, unsigned& n_waits) {
     using RG = typename Types<P>::Ring;
     using FT = typename Types<P>::Flux;
     using RT = typename Types<P>::Math;
-    using C = Tile<P>;
+    using C = Tile<P, SK>;
     constexpr int TX = C::TX, TY = C::TY, NC = C::NC, NT = C::NT, HX = C::HX, PLANE = C::PLANE;
     constexpr int NXF = C::NXF, NYF = C::NYF;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -408,9 +408,9 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         if (use_tma) {
             if (!mbar_wait_bounded(bar, n_waits & 1u)) atomicAdd(&A.st->n_timeout, 1ull);
             n_waits++;
-            convert_plane<P, RG>(A, stg, slot, i0, j0);
+            convert_plane<P, SK, RG>(A, stg, slot, i0, j0);
         } else {
-            load_plane<P, RG>(A, slot, i0, j0, kk);
+            load_plane<P, SK, RG>(A, slot, i0, j0, kk);
         }
         __syncthreads();
         if (use_tma && t == 0 && kk < kz_last) issue_copy(kk + 1);
@@ -551,20 +551,20 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) stage_kernel(const StageArgs A) {
+__global__ void __launch_bounds__(Tile<P, KIND>::NT, Tile<P, KIND>::MINB) stage_kernel(const StageArgs A) {
     __shared__ __align__(8) unsigned long long bar;
     if (threadIdx.x == 0) mbar_init(&bar);
     __syncthreads();
     unsigned n_waits = 0;
-    run_tile<P, NSTATE, ORDER, KIND, WANT_DT>(A, blockIdx.x, blockIdx.y, blockIdx.z,
-                                               gridDim.x * gridDim.y * gridDim.z, &bar, n_waits);
+    run_tile<P, NSTATE, ORDER, KIND, WANT_DT, KIND>(A, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                     gridDim.x * gridDim.y * gridDim.z, &bar, n_waits);
 }
 
 // Persistent batch kernel: each CTA takes tiles from the work queue until it is empty; the
 // tile's solve selects the arguments (copied to shared memory) and the Riemann solver.  The
 // items of one solve are counted by its own clock, so every solve keeps its own lagged dt.
 template <int P, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) batch_stage_kernel(const BatchArgs B) {
+__global__ void __launch_bounds__(Tile<P, 1>::NT, Tile<P, 1>::MINB) batch_stage_kernel(const BatchArgs B) {
     __shared__ __align__(16) StageArgs As;
     __shared__ int4 it;
     __shared__ __align__(8) unsigned long long bar;
@@ -582,35 +582,36 @@ __global__ void __launch_bounds__(Tile<P>::NT, Tile<P>::MINB) batch_stage_kernel
         if (w.x < 0) break;
         const unsigned long long* src = reinterpret_cast<const unsigned long long*>(B.inst + w.x);
         unsigned long long* dst = reinterpret_cast<unsigned long long*>(&As);
-        for (int q = threadIdx.x; q < WORDS; q += Tile<P>::NT) dst[q] = src[q];
+        for (int q = threadIdx.x; q < WORDS; q += Tile<P, 1>::NT) dst[q] = src[q];
         __syncthreads();
         if (As.n_state == 3)
-            run_tile<P, 3, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
+            run_tile<P, 3, ORDER, KIND, WANT_DT, 1>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
         else
-            run_tile<P, 2, ORDER, KIND, WANT_DT>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
+            run_tile<P, 2, ORDER, KIND, WANT_DT, 1>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
     }
 }
 
 // Dynamic shared memory: alignment slack, staged box (FP64), primitive ring, x / y flux buffers.
-template <int P>
+template <int P, int SK>
 constexpr int smem_bytes() {
-    return 128 + 8 * Tile<P>::PLANE * (int)sizeof(double) + RING * 8 * Tile<P>::PLANE * (int)sizeof(typename Types<P>::Ring) +
-           8 * (Tile<P>::NXF + Tile<P>::NYF) * (int)sizeof(typename Types<P>::Flux);
+    using C = Tile<P, SK>;
+    return 128 + 8 * C::PLANE * (int)sizeof(double) + RING * 8 * C::PLANE * (int)sizeof(typename Types<P>::Ring) +
+           8 * (C::NXF + C::NYF) * (int)sizeof(typename Types<P>::Flux);
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
     auto kern = stage_kernel<P, NSTATE, ORDER, KIND, WANT_DT>;
-    const int smem = smem_bytes<P>();
+    const int smem = smem_bytes<P, KIND>();
     static bool attr_set = false;   // per process; every device shares the same limit
     if (!attr_set) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    constexpr int TX = Tile<P>::TX, TY = Tile<P>::TY;
+    constexpr int TX = Tile<P, KIND>::TX, TY = Tile<P, KIND>::TY;
     dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, (a.g.nz + a.g.lz - 1) / a.g.lz);
-    kern<<<grid, Tile<P>::NT, smem, s>>>(a);
+    kern<<<grid, Tile<P, KIND>::NT, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -637,7 +638,7 @@ cudaError_t launch_p(const StageArgs& a, int n_state, int order, int kind, bool 
 template <int P, int KIND, bool WANT_DT>
 cudaError_t batch_attr() {
     return cudaFuncSetAttribute(batch_stage_kernel<P, 2, KIND, WANT_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem_bytes<P>());
+                                smem_bytes<P, 1>());
 }
 
 }  // namespace
@@ -656,13 +657,13 @@ cudaError_t prepare_batch_kernels(int precision) {
     return batch_attr<0, 1, false>();
 }
 
-int batch_ctas_per_sm(int precision) { return tile_shape(precision).ctas_per_sm; }
+int batch_ctas_per_sm(int precision) { return tile_shape(precision, 1).ctas_per_sm; }
 
 template <int P>
 void launch_batch_p(const BatchArgs& b, int kind, bool want_dt, int grid, cudaStream_t s) {
-    constexpr int NT = Tile<P>::NT;
-    if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P>(), s>>>(b);
-    else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P>(), s>>>(b);
+    constexpr int NT = Tile<P, 1>::NT;
+    if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P, 1>(), s>>>(b);
+    else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P, 1>(), s>>>(b);
 }
 
 cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
@@ -673,10 +674,11 @@ cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool
     return cudaGetLastError();
 }
 
-int stage_smem_bytes(int precision) {
-    return precision == 1 ? smem_bytes<1>() : (precision == 2 ? smem_bytes<2>() : smem_bytes<0>());
+int stage_smem_bytes(int precision, int kind) {
+    if (precision == 1) return kind == 0 ? smem_bytes<1, 0>() : smem_bytes<1, 1>();
+    return precision == 2 ? smem_bytes<2, 0>() : smem_bytes<0, 0>();
 }
-int stage_fp64_smem_bytes() { return smem_bytes<0>(); }
+int stage_fp64_smem_bytes() { return smem_bytes<0, 0>(); }
 
 cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
                          cudaStream_t s) {
