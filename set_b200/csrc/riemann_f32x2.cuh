@@ -29,6 +29,33 @@ __device__ __forceinline__ F2 rsqrt2(F2 a) { return F2{sb_rsqrt(a.x), sb_rsqrt(a
 __device__ __forceinline__ F2 pos2(F2 a) { return F2{fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)}; }
 __device__ __forceinline__ float pick(F2 a, bool right) { return right ? a.y : a.x; }
 
+// minmod of each lane (the branch-free FP32 form of mhd_core.cuh's minmod)
+__device__ __forceinline__ F2 minmod2(F2 a, F2 b) { return F2{minmod(a.x, b.x), minmod(a.y, b.y)}; }
+
+// The MUSCL-minmod face states of both sides at once (reconstruct() of mhd_core.cuh, second
+// order): side L is t_c + 0.5*minmod(t_c - t_f, t_n - t_c) with (t_f, t_c, t_n) = (LL, L, R),
+// side R the same with (RR, R, L); each variable's two sides are one f32x2 pair.  Positivity
+// fallback of cuf_solvers.cuf:394-406; B stays first order.
+__device__ __forceinline__ void reconstruct_f32x2(const float* qLL, const float* qL, const float* qR,
+                                                  const float* qRR, float* q1, float* q2) {
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+        q1[v] = qL[v];
+        q2[v] = qR[v];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        const F2 c = mk(qL[v], qR[v]), fa = mk(qLL[v], qRR[v]), ne = mk(qR[v], qL[v]);
+        const F2 r = fma2(splat(0.5f), minmod2(c - fa, ne - c), c);
+        q1[v] = r.x;
+        q2[v] = r.y;
+    }
+    if (q1[0] < 0.0f) q1[0] = qL[0];
+    if (q1[4] < 0.0f) q1[4] = qL[4];
+    if (q2[0] < 0.0f) q2[0] = qR[0];
+    if (q2[4] < 0.0f) q2[4] = qR[4];
+}
+
 // Face-frame states q = (rho, vn, vt1, vt2, p, Bn, Bt1, Bt2), B in stored units; F in the same
 // order (B fluxes in stored units); SL, SR, SM as chlld's dsl, dsp, dsc.  Returns kFlagWave when
 // no wave-fan region matched and kFlagStar when the selected state has rho <= 0 or p <= 0 or

@@ -336,7 +336,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             real = (i0 + fxx < g.nx) && (j0 + fyy <= g.ny);
         }
         RT q1[8], q2[8], F[8];
-        reconstruct<RT, ORDER>(qLL, qL, qR, qRR, q1, q2);
+        if constexpr (P == 1 && ORDER == 2) reconstruct_f32x2(qLL, qL, qR, qRR, q1, q2);
+        else reconstruct<RT, ORDER>(qLL, qL, qR, qRR, q1, q2);
         if (real && !dup && (q1[0] < RT(0) || q2[0] < RT(0))) n_recon++;
         int fl;
         double sl, sr;
