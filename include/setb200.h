@@ -121,6 +121,30 @@ SETB_API int32_t setb_chlld_batch(int64_t n, int32_t n_state, int32_t n_disc, in
                          const double* normals, const double* w, const double* q1, const double* q2,
                          double* qqq, double* speeds, int32_t* flags);
 
+/* ------------------------------------------------------------------ passive-scalar flux routine
+ * Replaces: subroutine chlld_Q(n_state, al, be, ge, w, qqq1, qqq2, dsl, dsp, dsc, qqq, null_bn1,
+ *           n_disc, p_correct_, konvect_, ydar_)   SET_Fortran_Cuda_MHD/Solvers.f90:198-201
+ * chlld with a ninth, passively advected variable Q = qqq(9) and an optional second scalar.
+ * Fortran calling convention (all by reference); the OPTIONAL arguments null_bn1, n_disc,
+ * p_correct_, konvect_ and ydar_ may be NULL.  Fortran LOGICALs are passed as int32 (nonzero =
+ * .TRUE.).  null_bn1 and p_correct_ are accepted and, as in the reference (:266-267), change
+ * nothing.  konvect_ is the (3,1) array: [0], [1] the scalar's left / right values (in), [2] its
+ * flux (out).  ydar_ = .TRUE. takes the left-state branch of the wave fan (:550, :698, :951).
+ * Returns SETB_EWAVES where the reference prints and STOPs.  Runs on the host. */
+SETB_API int32_t setb_chlld_q(const int32_t* n_state, const double* al, const double* be, const double* ge,
+                     const double* w, const double qqq1[9], const double qqq2[9], double* dsl,
+                     double* dsp, double* dsc, double qqq[9], const int32_t* null_bn1,
+                     const int32_t* n_disc, const int32_t* p_correct_, double* konvect_,
+                     const int32_t* ydar_);
+
+/* Batched chlld_Q on the GPU (FP64): n faces, host arrays; face k uses normals[3k..3k+2], w[k]
+ * (NULL = 0), q1[9k..], q2[9k..]; konvect (NULL = absent) holds 3 values per face, [3k], [3k+1]
+ * in and [3k+2] out.  Writes qqq[9k..], speeds[3k..] = (dsl, dsp, dsc), flags[k] (0 ok, 1 no
+ * wave-fan region matched). */
+SETB_API int32_t setb_chlld_q_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t ydar,
+                           const double* normals, const double* w, const double* q1, const double* q2,
+                           double* konvect, double* qqq, double* speeds, int32_t* flags);
+
 /* ------------------------------------------------------------------ device-resident solver
  * Replaces Set_CUDA (cuf_kernel.cuf:351-382): allocate device state and upload Cell_par. */
 SETB_API int32_t setb_init_cartesian(setb_handle** h, const setb_cart_desc* d, const double* cell_par);

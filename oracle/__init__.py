@@ -67,6 +67,9 @@ def lib():
         _lib.orc_chlld.restype = C.c_int
         _lib.orc_chlld.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp,
                                    _dp, _dp, _dp, _dp, C.c_int]
+        _lib.orc_chlld_q.restype = C.c_int
+        _lib.orc_chlld_q.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp,
+                                     _dp, _dp, _dp, _dp, C.c_int, C.c_int, _dp]
         _lib.orc_minmod.restype = C.c_double
         _lib.orc_minmod.argtypes = [C.c_double, C.c_double]
         _lib.orc_linear.restype = C.c_double
@@ -113,6 +116,22 @@ def chlld(n_state, normal, w, q1, q2, n_disc=0):
     rc = lib().orc_chlld(int(n_state), float(normal[0]), float(normal[1]), float(normal[2]), float(w),
                          _p(q1), _p(q2), C.byref(dsl), C.byref(dsp), C.byref(dsc), _p(out), int(n_disc))
     return rc, out, dsl.value, dsp.value, dsc.value
+
+
+def chlld_q(n_state, normal, w, q1, q2, n_disc=0, ydar=False, konvect=None):
+    """Scalar chlld_Q (Solvers.f90:198-1141): q1/q2 are 9-vectors (Q last).  konvect is None or
+    (left, right) of the second passive scalar.  Returns (status, qqq[9], dsl, dsp, dsc, kflux)
+    with kflux None when konvect is None."""
+    q1 = np.ascontiguousarray(q1, dtype=np.float64)
+    q2 = np.ascontiguousarray(q2, dtype=np.float64)
+    assert q1.shape == (9,) and q2.shape == (9,)
+    out = np.zeros(9)
+    kv = None if konvect is None else np.array([konvect[0], konvect[1], 0.0])
+    dsl, dsp, dsc = C.c_double(), C.c_double(), C.c_double()
+    rc = lib().orc_chlld_q(int(n_state), float(normal[0]), float(normal[1]), float(normal[2]), float(w),
+                           _p(q1), _p(q2), C.byref(dsl), C.byref(dsp), C.byref(dsc), _p(out), int(n_disc),
+                           int(bool(ydar)), None if kv is None else _p(kv))
+    return rc, out, dsl.value, dsp.value, dsc.value, (None if kv is None else kv[2])
 
 
 def ref_hll(normal, w, q1, q2, dist=1.0):

@@ -8,6 +8,7 @@
 //
 // What it restates (paths are inside the reference project):
 //   * chlld, all four n_state branches and n_disc 0/1/2 ........ SET_Fortran_Cuda_MHD/Solvers.f90:1144-1859
+//   * chlld_Q (chlld + passive scalar Q + konvect_ scalar + ydar) SET_Fortran_Cuda_MHD/Solvers.f90:198-1141
 //   * signum / minmod / linear ................................. SET_Fortran_Cuda_MHD/Solvers.f90:109-150
 //   * face semantics (TVD of vars 1..5, positivity fallback, dt candidate, flux*square)
 //                                                                SET_Fortran_Cuda_MHD/cuf_solvers.cuf:243-440
@@ -518,6 +519,465 @@ int chlld(int n_state, double al, double be, double ge, double w, const double* 
     return 0;   // n_state > 3: the reference leaves qqq untouched
 }
 
+// ---------------------------------------------------------------- Solvers.f90:198-1141
+// chlld_Q: chlld with a ninth, passively advected variable Q (qqq(9), :293, :303) and an
+// optional second passive scalar in konvect_(3,1) = (left value, right value, flux out).  What
+// changes results against chlld: epsb = 1e-4 (:282); the n_disc = 2 blend weight 0.60 (:432);
+// the HLLC star total pressure by the HLLD formula (:639); the HLL and HLLC wave-fan selection
+// as else-if chains that STOP when nothing matched (:550-587, :698-774); `ydar`, which forces
+// the left-state branch (:550, :698, :951).  null_bn1 and p_correct_ are read and then
+// overridden (phi_p_correct = 1.0 at :266, null_bn = .False. at :267): they have no effect.
+// kv is NULL when konvect_ is absent, else kv[0..2] = konvect_(1..3, 1); the declared shape
+// (3, 1) makes size(konvect_(1, :)) = 1.
+// Returns 0, or 1 when no wave-fan region matched (the reference prints and STOPs).
+int chlld_q(int n_state, double al, double be, double ge, double w, const double* qqq1,
+            const double* qqq2, double& dsl, double& dsp, double& dsc, double* qqq, int n_disc,
+            bool ydar, double* kv) {
+    const double x0 = 0., x1 = 1., x2 = 2., x3 = 3., x5 = 5.;
+    double FR[9], FL[9], FW[9], UL[9], UZ[9], UR[9], UZL[9], UZR[9], UZZL[9], UZZR[9], dq[9];
+    double vL[3], vR[3], bL[3], bR[3], vzL[3], vzR[3], bzL[3], bzR[3];
+    double vzzL[3], vzzR[3], bzzL[3], bzzR[3], aco[3][3], qv[3], qb[3];
+    double FL_ = 0.0, FR_ = 0.0, UZ_ = 0.0, FW_ = 0.0;
+
+    const int n_disco = n_disc;                    // :269-273
+    const double spi4 = std::sqrt(cpi4);           // :279
+    const double eps = 1.0e-12;                    // :281
+    const double epsb = 1.0e-04;                   // :282
+    const double ga = x5 / x3;                     // :287
+    const double g1 = ga - x1;
+    const double wv = w;
+
+    const double q1 = qqq1[8], r1 = qqq1[0], u1 = qqq1[1], v1 = qqq1[2], w1 = qqq1[3], p1 = qqq1[4];
+    const double bx1 = qqq1[5] / spi4, by1 = qqq1[6] / spi4, bz1 = qqq1[7] / spi4;
+    const double q2 = qqq2[8], r2 = qqq2[0], u2 = qqq2[1], v2 = qqq2[2], w2 = qqq2[3], p2 = qqq2[4];
+    const double bx2 = qqq2[5] / spi4, by2 = qqq2[6] / spi4, bz2 = qqq2[7] / spi4;
+
+    const double ro = (r2 + r1) / x2;              // :313-320
+    const double ap = (p2 + p1) / x2;
+    const double abx = (bx2 + bx1) / x2, aby = (by2 + by1) / x2, abz = (bz2 + bz1) / x2;
+
+    const double bk = abx * al + aby * be + abz * ge;   // :323-360
+    const double b2 = abx * abx + aby * aby + abz * abz;
+    double d = b2 - bk * bk;
+    aco[0][0] = al;
+    aco[1][0] = be;
+    aco[2][0] = ge;
+    if (d > eps) {
+        d = std::sqrt(d);
+        aco[0][1] = (abx - bk * al) / d;
+        aco[1][1] = (aby - bk * be) / d;
+        aco[2][1] = (abz - bk * ge) / d;
+        aco[0][2] = (aby * ge - abz * be) / d;
+        aco[1][2] = (abz * al - abx * ge) / d;
+        aco[2][2] = (abx * be - aby * al) / d;
+    } else {
+        double aix, aiy, aiz;
+        if (std::fabs(al) < std::fabs(be) && std::fabs(al) < std::fabs(ge)) {
+            aix = x1; aiy = x0; aiz = x0;
+        } else if (std::fabs(be) < std::fabs(ge)) {
+            aix = x0; aiy = x1; aiz = x0;
+        } else {
+            aix = x0; aiy = x0; aiz = x1;
+        }
+        const double aik = aix * al + aiy * be + aiz * ge;
+        d = std::sqrt(x1 - aik * aik);
+        aco[0][1] = (aix - aik * al) / d;
+        aco[1][1] = (aiy - aik * be) / d;
+        aco[2][1] = (aiz - aik * ge) / d;
+        aco[0][2] = (aiy * ge - aiz * be) / d;
+        aco[1][2] = (aiz * al - aix * ge) / d;
+        aco[2][2] = (aix * be - aiy * al) / d;
+    }
+    for (int i = 0; i < 3; i++) {                  // :363-368
+        vL[i] = aco[0][i] * u1 + aco[1][i] * v1 + aco[2][i] * w1;
+        vR[i] = aco[0][i] * u2 + aco[1][i] * v2 + aco[2][i] * w2;
+        bL[i] = aco[0][i] * bx1 + aco[1][i] * by1 + aco[2][i] * bz1;
+        bR[i] = aco[0][i] * bx2 + aco[1][i] * by2 + aco[2][i] * bz2;
+    }
+
+    const double aaL = bL[0] / std::sqrt(r1);      // :370-394
+    const double b2L = bL[0] * bL[0] + bL[1] * bL[1] + bL[2] * bL[2];
+    const double b21 = b2L / r1;
+    const double cL = std::sqrt(ga * p1 / r1);
+    double qp = std::sqrt(b21 + cL * (cL + x2 * aaL));
+    double qm = std::sqrt(b21 + cL * (cL - x2 * aaL));
+    const double cfL = (qp + qm) / x2;
+    const double ptL = p1 + b2L / x2;
+    const double aaR = bR[0] / std::sqrt(r2);
+    const double b2R = bR[0] * bR[0] + bR[1] * bR[1] + bR[2] * bR[2];
+    const double b22 = b2R / r2;
+    const double cR = std::sqrt(ga * p2 / r2);
+    qp = std::sqrt(b22 + cR * (cR + x2 * aaR));
+    qm = std::sqrt(b22 + cR * (cR - x2 * aaR));
+    const double cfR = (qp + qm) / x2;
+    const double ptR = p2 + b2R / x2;
+    const double aC = (aaL + aaR) / x2;
+    const double b2o = (b22 + b21) / x2;
+    const double cC = std::sqrt(ga * ap / ro);
+    qp = std::sqrt(b2o + cC * (cC + x2 * aC));
+    qm = std::sqrt(b2o + cC * (cC - x2 * aC));
+    const double cfC = (qp + qm) / x2;
+    const double vC1 = (vL[0] + vR[0]) / x2;
+
+    double SL = 0.0, SR = 0.0;                     // :413-436
+    if (n_disco == 1) {
+        SL = std::min((vL[0] - cfL), (vC1 - cfC));
+        SR = std::max((vR[0] + cfR), (vC1 + cfC));
+    }
+    if (n_disco == 0) {
+        SL = std::min((vL[0] - cfL), (vR[0] - cfR));
+        SR = std::max((vL[0] + cfL), (vR[0] + cfR));
+    }
+    if (n_disco == 2) {
+        const double SL_1 = std::min((vL[0] - cfL), (vC1 - cfC));
+        const double SR_1 = std::max((vR[0] + cfR), (vC1 + cfC));
+        const double SL_2 = std::min((vL[0] - cfL), (vR[0] - cfR));
+        const double SR_2 = std::max((vL[0] + cfL), (vR[0] + cfR));
+        const double oo = 0.60;
+        const double oo1 = 1.0 - oo;
+        SL = oo * SL_1 + oo1 * SL_2;
+        SR = oo * SR_1 + oo1 * SR_2;
+    }
+
+    const double suR = SR - vR[0];                 // :447-454
+    const double suL = SL - vL[0];
+    const double SM = (suR * r2 * vR[0] - ptR + ptL - suL * r1 * vL[0]) / (suR * r2 - suL * r1);
+    dsl = SL;
+    dsc = SM;
+    dsp = SR;
+
+    if (n_state == 0) {                            // :466-471
+        const double TR0 = std::fabs(vL[0] + vR[0]) / x2 + cfC;
+        SR = TR0;
+        SL = -TR0;
+    }
+
+    const double upt1 = (u1 * u1 + v1 * v1 + w1 * w1) / x2;   // :474-481
+    const double sbv1 = u1 * bx1 + v1 * by1 + w1 * bz1;
+    const double upt2 = (u2 * u2 + v2 * v2 + w2 * w2) / x2;
+    const double sbv2 = u2 * bx2 + v2 * by2 + w2 * bz2;
+    const double e1 = p1 / g1 + r1 * upt1 + b2L / x2;
+    const double e2 = p2 / g1 + r2 * upt2 + b2R / x2;
+
+    FL[0] = r1 * vL[0];                            // :483-511
+    FL[8] = q1 * vL[0];
+    FL[1] = r1 * vL[0] * vL[0] + ptL - bL[0] * bL[0];
+    FL[2] = r1 * vL[0] * vL[1] - bL[0] * bL[1];
+    FL[3] = r1 * vL[0] * vL[2] - bL[0] * bL[2];
+    FL[4] = (e1 + ptL) * vL[0] - bL[0] * sbv1;
+    FL[5] = x0;
+    FL[6] = vL[0] * bL[1] - vL[1] * bL[0];
+    FL[7] = vL[0] * bL[2] - vL[2] * bL[0];
+    if (kv) FL_ = kv[0] * vL[0];
+    FR[0] = r2 * vR[0];
+    FR[8] = q2 * vR[0];
+    FR[1] = r2 * vR[0] * vR[0] + ptR - bR[0] * bR[0];
+    FR[2] = r2 * vR[0] * vR[1] - bR[0] * bR[1];
+    FR[3] = r2 * vR[0] * vR[2] - bR[0] * bR[2];
+    FR[4] = (e2 + ptR) * vR[0] - bR[0] * sbv2;
+    FR[5] = x0;
+    FR[6] = vR[0] * bR[1] - vR[1] * bR[0];
+    FR[7] = vR[0] * bR[2] - vR[2] * bR[0];
+    if (kv) FR_ = kv[1] * vR[0];
+
+    UL[0] = r1;                                    // :513-524
+    UL[8] = q1;
+    UL[4] = e1;
+    UR[0] = r2;
+    UR[8] = q2;
+    UR[4] = e2;
+    for (int ik = 0; ik < 3; ik++) {
+        UL[ik + 1] = r1 * vL[ik];
+        UL[ik + 5] = bL[ik];
+        UR[ik + 1] = r2 * vR[ik];
+        UR[ik + 5] = bR[ik];
+    }
+    for (int ik = 0; ik < 9; ik++)                 // :526-528
+        UZ[ik] = (SR * UR[ik] - SL * UL[ik] + FL[ik] - FR[ik]) / (SR - SL);
+    if (kv) UZ_ = (SR * kv[1] - SL * kv[0] + FL_ - FR_) / (SR - SL);   // :530-534
+
+    if (n_state <= 1) {                            // :541-621  HLL / Lax
+        for (int ik = 0; ik < 9; ik++) dq[ik] = UR[ik] - UL[ik];
+        double TL = SL, TR = SR;
+        if (SL > wv || ydar) {
+            TL = x0;
+            for (int ik = 0; ik < 9; ik++) FW[ik] = wv * UL[ik];
+            if (kv) FW_ = wv * kv[0];
+        } else if (SL <= wv && wv <= SR) {
+            for (int ik = 0; ik < 9; ik++) FW[ik] = wv * UZ[ik];
+            if (kv) FW_ = wv * UZ_;
+        } else if (SR < wv) {
+            TR = x0;
+            for (int ik = 0; ik < 9; ik++) FW[ik] = wv * UR[ik];
+            if (kv) FW_ = wv * kv[1];
+        } else {
+            return 1;                              // :584-587
+        }
+        const double a = TR * TL;
+        const double b = TR - TL;
+        qqq[0] = (TR * FL[0] - TL * FR[0] + a * dq[0]) / b - FW[0];
+        qqq[8] = (TR * FL[8] - TL * FR[8] + a * dq[8]) / b - FW[8];
+        qqq[4] = (TR * FL[4] - TL * FR[4] + a * dq[4]) / b - FW[4];
+        for (int ik = 1; ik < 4; ik++) qv[ik - 1] = (TR * FL[ik] - TL * FR[ik] + a * dq[ik]) / b - FW[ik];
+        for (int ik = 5; ik < 8; ik++) qb[ik - 5] = (TR * FL[ik] - TL * FR[ik] + a * dq[ik]) / b - FW[ik];
+        for (int i = 0; i < 3; i++) {
+            qqq[i + 1] = aco[i][0] * qv[0] + aco[i][1] * qv[1] + aco[i][2] * qv[2];
+            qqq[i + 5] = aco[i][0] * qb[0] + aco[i][1] * qb[1] + aco[i][2] * qb[2];
+            qqq[i + 5] = spi4 * qqq[i + 5];
+        }
+        if (kv) kv[2] = (TR * FL_ - TL * FR_ + a * (kv[1] - kv[0])) / b - FW_;   // :609-613
+        return 0;
+    }
+
+    if (n_state == 2) {                            // :624-812  HLLC
+        const double suRm = suR / (SR - SM);
+        const double suLm = suL / (SL - SM);
+        const double rzR = r2 * suRm, rzL = r1 * suLm;
+        const double qzR = q2 * suRm, qzL = q1 * suLm;
+        vzR[0] = SM;
+        vzL[0] = SM;
+        const double ptz = (suR * r2 * ptL - suL * r1 * ptR + 1.0 * r1 * r2 * suR * suL * (vR[0] - vL[0])) /
+                           (suR * r2 - suL * r1);  // :639-640, phi_p_correct = 1
+        bzR[0] = UZ[5];
+        bzL[0] = UZ[5];
+        // :645-648 assign UZ(3)/UZ(1), UZ(4)/UZ(1), overwritten at :651-654
+        vzR[1] = vR[1] + UZ[5] * (bR[1] - UZ[6]) / suR / r2;
+        vzR[2] = vR[2] + UZ[5] * (bR[2] - UZ[7]) / suR / r2;
+        vzL[1] = vL[1] + UZ[5] * (bL[1] - UZ[6]) / suL / r1;
+        vzL[2] = vL[2] + UZ[5] * (bL[2] - UZ[7]) / suL / r1;
+        bzR[1] = UZ[6];
+        bzR[2] = UZ[7];
+        bzL[1] = bzR[1];
+        bzL[2] = bzR[2];
+        const double sbvz = (UZ[5] * UZ[1] + UZ[6] * UZ[2] + UZ[7] * UZ[3]) / UZ[0];
+        const double ezR = e2 * suRm + (ptz * SM - ptR * vR[0] + UZ[5] * (sbv2 - sbvz)) / (SR - SM);
+        const double ezL = e1 * suLm + (ptz * SM - ptL * vL[0] + UZ[5] * (sbv1 - sbvz)) / (SL - SM);
+        if (std::fabs(UZ[5]) < epsb) {             // :666-675
+            vzR[1] = vR[1];
+            vzR[2] = vR[2];
+            vzL[1] = vL[1];
+            vzL[2] = vL[2];
+            bzR[1] = bR[1] * suRm;
+            bzR[2] = bR[2] * suRm;
+            bzL[1] = bL[1] * suLm;
+            bzL[2] = bL[2] * suLm;
+        }
+        UZL[0] = rzL;                              // :684-696
+        UZL[8] = qzL;
+        UZL[4] = ezL;
+        UZR[0] = rzR;
+        UZR[8] = qzR;
+        UZR[4] = ezR;
+        for (int ik = 0; ik < 3; ik++) {
+            UZL[ik + 1] = vzL[ik] * rzL;
+            UZL[ik + 5] = bzL[ik];
+            UZR[ik + 1] = vzR[ik] * rzR;
+            UZR[ik + 5] = bzR[ik];
+        }
+        if (SL >= wv || ydar) {                    // :698-774
+            qqq[0] = FL[0] - wv * UL[0];
+            qqq[8] = FL[8] - wv * UL[8];
+            qqq[4] = FL[4] - wv * UL[4];
+            for (int ik = 1; ik < 4; ik++) qv[ik - 1] = FL[ik] - wv * UL[ik];
+            for (int ik = 5; ik < 8; ik++) qb[ik - 5] = FL[ik] - wv * UL[ik];
+            if (kv) kv[2] = FL_ - wv * kv[0];
+        } else if (SL <= wv && SM >= wv) {
+            qqq[0] = FL[0] + SL * (rzL - r1) - wv * UZL[0];
+            qqq[8] = FL[8] + SL * (qzL - q1) - wv * UZL[8];
+            qqq[4] = FL[4] + SL * (ezL - e1) - wv * UZL[4];
+            for (int ik = 1; ik < 4; ik++) qv[ik - 1] = FL[ik] + SL * (UZL[ik] - UL[ik]) - wv * UZL[ik];
+            for (int ik = 5; ik < 8; ik++) qb[ik - 5] = FL[ik] + SL * (UZL[ik] - UL[ik]) - wv * UZL[ik];
+            if (kv) kv[2] = FL_ + SL * (kv[0] * suLm - kv[0]) - wv * kv[0] * suLm;
+        } else if (SM <= wv && SR >= wv) {
+            qqq[0] = FR[0] + SR * (rzR - r2) - wv * UZR[0];
+            qqq[8] = FR[8] + SR * (qzR - q2) - wv * UZR[8];
+            qqq[4] = FR[4] + SR * (ezR - e2) - wv * UZR[4];
+            for (int ik = 1; ik < 4; ik++) qv[ik - 1] = FR[ik] + SR * (UZR[ik] - UR[ik]) - wv * UZR[ik];
+            for (int ik = 5; ik < 8; ik++) qb[ik - 5] = FR[ik] + SR * (UZR[ik] - UR[ik]) - wv * UZR[ik];
+            if (kv) kv[2] = FR_ + SR * (kv[1] * suRm - kv[1]) - wv * kv[1] * suRm;
+        } else if (SR < wv) {
+            qqq[0] = FR[0] - wv * UR[0];
+            qqq[8] = FR[8] - wv * UR[8];
+            qqq[4] = FR[4] - wv * UR[4];
+            for (int ik = 1; ik < 4; ik++) qv[ik - 1] = FR[ik] - wv * UR[ik];
+            for (int ik = 5; ik < 8; ik++) qb[ik - 5] = FR[ik] - wv * UR[ik];
+            if (kv) kv[2] = FR_ - wv * kv[1];
+        } else {
+            return 1;                              // :769-774
+        }
+        const double SN = std::max(std::fabs(SL), std::fabs(SR));   // :777-790
+        double wbn = x0;
+        if (wv >= SR) wbn = wv * bR[0];
+        else if (wv <= SL) wbn = wv * bL[0];
+        else wbn = wv * (bL[0] + bR[0]) / x2;
+        qb[0] = -SN * (bR[0] - bL[0]) - wbn;
+        for (int i = 0; i < 3; i++) {              // :796-803
+            qqq[i + 1] = aco[i][0] * qv[0] + aco[i][1] * qv[1] + aco[i][2] * qv[2];
+            qqq[i + 5] = aco[i][0] * qb[0] + aco[i][1] * qb[1] + aco[i][2] * qb[2];
+            qqq[i + 5] = spi4 * qqq[i + 5];
+        }
+        return 0;
+    }
+
+    if (n_state == 3) {                            // :815-1136  HLLD
+        const double ptz = (suR * r2 * ptL - suL * r1 * ptR + 1.0 * r1 * r2 * suR * suL * (vR[0] - vL[0])) /
+                           (suR * r2 - suL * r1);
+        vzL[0] = SM;
+        vzR[0] = SM;
+        vzzL[0] = SM;
+        vzzR[0] = SM;
+        const double suRm = suR / (SR - SM);
+        const double suLm = suL / (SL - SM);
+        const double rzR = r2 * suRm, rzL = r1 * suLm;
+        const double qzR = q2 * suRm, qzL = q1 * suLm;
+        const double bn = UZ[5];
+        const double bn2 = bn * bn;
+        bzL[0] = bn;
+        bzR[0] = bn;
+        bzzL[0] = bn;
+        bzzR[0] = bn;
+        double tvR, tbR, tvL, tbL;
+        const double ttR = r2 * suR * (SR - SM) - bn2;   // :843-860
+        if (std::fabs(ttR) <= 1.0e-09) {
+            tvR = x0;
+            tbR = x0;
+        } else {
+            tvR = (SM - vR[0]) / ttR;
+            tbR = (r2 * suR * suR - bn2) / ttR;
+        }
+        const double ttL = r1 * suL * (SL - SM) - bn2;
+        if (std::fabs(ttL) <= 1.0e-09) {
+            tvL = x0;
+            tbL = x0;
+        } else {
+            tvL = (SM - vL[0]) / ttL;
+            tbL = (r1 * suL * suL - bn2) / ttL;
+        }
+        vzL[1] = vL[1] - bn * bL[1] * tvL;
+        vzL[2] = vL[2] - bn * bL[2] * tvL;
+        vzR[1] = vR[1] - bn * bR[1] * tvR;
+        vzR[2] = vR[2] - bn * bR[2] * tvR;
+        bzL[1] = bL[1] * tbL;
+        bzL[2] = bL[2] * tbL;
+        bzR[1] = bR[1] * tbR;
+        bzR[2] = bR[2] * tbR;
+        const double sbvL = bzL[0] * vzL[0] + bzL[1] * vzL[1] + bzL[2] * vzL[2];
+        const double sbvR = bzR[0] * vzR[0] + bzR[1] * vzR[1] + bzR[2] * vzR[2];
+        const double ezR = e2 * suRm + (ptz * SM - ptR * vR[0] + bn * (sbv2 - sbvR)) / (SR - SM);
+        const double ezL = e1 * suLm + (ptz * SM - ptL * vL[0] + bn * (sbv1 - sbvL)) / (SL - SM);
+        const double rzzR = rzR, rzzL = rzL;       // :877-888 (the Q square roots there are unused)
+        const double qzzR = qzR, qzzL = qzL;
+        const double rzRs = std::sqrt(rzR);
+        const double rzLs = std::sqrt(rzL);
+        const double rzss = rzRs + rzLs;
+        const double rzps = rzRs * rzLs;
+        double SZL = SM - std::fabs(bn) / rzLs;    // :890-902
+        double SZR = SM + std::fabs(bn) / rzRs;
+        int ibn;
+        double sbn;
+        if (std::fabs(bn) > epsb) {
+            sbn = std::fabs(bn) / bn;
+            ibn = 1;
+        } else {
+            sbn = x0;
+            ibn = 0;
+            SZL = SM;
+            SZR = SM;
+        }
+        vzzL[1] = (rzLs * vzL[1] + rzRs * vzR[1] + sbn * (bzR[1] - bzL[1])) / rzss;
+        vzzL[2] = (rzLs * vzL[2] + rzRs * vzR[2] + sbn * (bzR[2] - bzL[2])) / rzss;
+        vzzR[1] = vzzL[1];
+        vzzR[2] = vzzL[2];
+        bzzL[1] = (rzLs * bzR[1] + rzRs * bzL[1] + sbn * rzps * (vzR[1] - vzL[1])) / rzss;
+        bzzL[2] = (rzLs * bzR[2] + rzRs * bzL[2] + sbn * rzps * (vzR[2] - vzL[2])) / rzss;
+        bzzR[1] = bzzL[1];
+        bzzR[2] = bzzL[2];
+        const double sbzz = bzzL[0] * vzzL[0] + bzzL[1] * vzzL[1] + bzzL[2] * vzzL[2];
+        const double ezzR = ezR + rzRs * sbn * (sbvR - sbzz);
+        const double ezzL = ezL - rzLs * sbn * (sbvL - sbzz);
+        UZL[0] = rzL;                              // :923-947
+        UZL[8] = qzL;
+        UZL[4] = ezL;
+        UZR[0] = rzR;
+        UZR[8] = qzR;
+        UZR[4] = ezR;
+        UZZL[0] = rzzL;
+        UZZL[8] = qzzL;
+        UZZL[4] = ezzL;
+        UZZR[0] = rzzR;
+        UZZR[8] = qzzR;
+        UZZR[4] = ezzR;
+        for (int ik = 0; ik < 3; ik++) {
+            UZL[ik + 1] = vzL[ik] * rzL;
+            UZL[ik + 5] = bzL[ik];
+            UZR[ik + 1] = vzR[ik] * rzR;
+            UZR[ik + 5] = bzR[ik];
+            UZZL[ik + 1] = vzzL[ik] * rzzL;
+            UZZL[ik + 5] = bzzL[ik];
+            UZZR[ik + 1] = vzzR[ik] * rzzR;
+            UZZR[ik + 5] = bzzR[ik];
+        }
+        // :949-1090.  Three selections, each of which overwrites the previous one's result:
+        // (L | L*) by an else-if chain with ydar forcing L, then (L** | R**) when the normal
+        // field is not degenerate, then (R* | R).  Vars 1, 9, 5 are written as qqq, 2..4 and
+        // 6..8 as the face-frame qv / qb.
+        int j_ccs = -1;
+        auto put = [&](int ik, double v) {
+            if (ik >= 1 && ik <= 3) qv[ik - 1] = v;
+            else if (ik >= 5 && ik <= 7) qb[ik - 5] = v;
+            else qqq[ik] = v;
+        };
+        if (SL >= wv || ydar) {
+            for (int ik = 0; ik < 9; ik++) put(ik, FL[ik] - wv * UL[ik]);
+            j_ccs = 1;
+            if (kv) kv[2] = FL_ - wv * kv[0];
+        } else if (SL <= wv && SZL >= wv) {
+            for (int ik = 0; ik < 9; ik++) put(ik, FL[ik] + SL * (UZL[ik] - UL[ik]) - wv * UZL[ik]);
+            j_ccs = 2;
+            if (kv) kv[2] = FL_ + SL * (kv[0] * suLm - kv[0]) - wv * kv[0] * suLm;
+        }
+        if (ibn == 1) {
+            if (SZL <= wv && SM >= wv) {
+                for (int ik = 0; ik < 9; ik++)
+                    put(ik, FL[ik] + SZL * (UZZL[ik] - UZL[ik]) + SL * (UZL[ik] - UL[ik]) - wv * UZZL[ik]);
+                j_ccs = 3;
+                if (kv) kv[2] = FL_ + SL * (kv[0] * suLm - kv[0]) - wv * kv[0] * suLm;
+            } else if (SM <= wv && SZR >= wv) {
+                for (int ik = 0; ik < 9; ik++)
+                    put(ik, FR[ik] + SZR * (UZZR[ik] - UZR[ik]) + SR * (UZR[ik] - UR[ik]) - wv * UZZR[ik]);
+                j_ccs = 4;
+                // :1042-1043 as written: the SZR term is SZR * (k2 suRm - k2 suRm)
+                if (kv)
+                    kv[2] = FR_ + SZR * (kv[1] * suRm - kv[1] * suRm) + SR * (kv[1] * suRm - kv[1]) -
+                            wv * kv[1] * suRm;
+            }
+        }
+        if (SZR <= wv && SR >= wv) {
+            for (int ik = 0; ik < 9; ik++) put(ik, FR[ik] + SR * (UZR[ik] - UR[ik]) - wv * UZR[ik]);
+            j_ccs = 5;
+            if (kv) kv[2] = FR_ + SR * (kv[1] * suRm - kv[1]) - wv * kv[1] * suRm;
+        } else if (SR < wv) {
+            for (int ik = 0; ik < 9; ik++) put(ik, FR[ik] - wv * UR[ik]);
+            j_ccs = 6;
+            if (kv) kv[2] = FR_ - wv * kv[1];
+        }
+        if (j_ccs == -1) return 1;                 // :1092-1104
+        const double SN = std::max(std::fabs(SL), std::fabs(SR));   // :1107-1121
+        double wbn = x0;
+        if (wv >= SR) wbn = wv * bR[0];
+        else if (wv <= SL) wbn = wv * bL[0];
+        else wbn = wv * (bL[0] + bR[0]) / x2;
+        qb[0] = -SN * (bR[0] - bL[0]) - wbn;
+        for (int i = 0; i < 3; i++) {              // :1125-1129
+            qqq[i + 1] = aco[i][0] * qv[0] + aco[i][1] * qv[1] + aco[i][2] * qv[2];
+            qqq[i + 5] = aco[i][0] * qb[0] + aco[i][1] * qb[1] + aco[i][2] * qb[2];
+            qqq[i + 5] = spi4 * qqq[i + 5];
+        }
+        return 0;
+    }
+    return 0;   // n_state > 3: qqq untouched
+}
+
 // ------------------------------------------------------------------ conserved <-> primitive
 // Conserved U = (rho, rho*u, rho*v, rho*w, E, Bx, By, Bz) with B in the reference's stored
 // units; the energy carries |b|^2/2 with b = B/sqrt(4*pi) as chlld does (Solvers.f90:1212-1214,
@@ -587,6 +1047,13 @@ typedef struct {
 int orc_chlld(int n_state, double al, double be, double ge, double w, const double* q1,
               const double* q2, double* dsl, double* dsp, double* dsc, double* qqq, int n_disc) {
     return chlld(n_state, al, be, ge, w, q1, q2, *dsl, *dsp, *dsc, qqq, n_disc);
+}
+
+// kv: NULL (konvect_ absent) or konvect_(1:3, 1) in / in / out
+int orc_chlld_q(int n_state, double al, double be, double ge, double w, const double* q1,
+                const double* q2, double* dsl, double* dsp, double* dsc, double* qqq, int n_disc, int ydar,
+                double* kv) {
+    return chlld_q(n_state, al, be, ge, w, q1, q2, *dsl, *dsp, *dsc, qqq, n_disc, ydar != 0, kv);
 }
 
 double orc_minmod(double x, double y) { return minmod(x, y); }

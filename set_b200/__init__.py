@@ -4,6 +4,7 @@ Python front end over the C ABI of libsetb200.so (include/setb200.h).  The names
 reference's solver-module interface:
 
     chlld(...)                  Solvers.f90:1144-1859 (host), chlld_batch(...) on the GPU
+    chlld_q(...)                Solvers.f90:198-1141 (host), chlld_q_batch(...) on the GPU
     Solver.init_cartesian(...)  Set_CUDA (cuf_kernel.cuf:351-382)
     Solver.step(n, opts)        the CUDA_START_MGD time loop (cuf_kernel.cuf:780-925)
     Solver.get_state()          Send_data_to_Host (cuf_kernel.cuf:384-400)
@@ -86,6 +87,9 @@ _SIGS = {
     "setb_chlld": (C.c_int32, [_ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip]),
     "setb_chlld_batch": (C.c_int32, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp,
                                      _dp, _dp, _ip]),
+    "setb_chlld_q": (C.c_int32, [_ip, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _dp, _ip]),
+    "setb_chlld_q_batch": (C.c_int32, [C.c_int64, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _dp,
+                                       _dp, _dp, _ip]),
     "setb_init_cartesian": (C.c_int32, [C.POINTER(C.c_void_p), C.POINTER(CartDesc), _dp]),
     "setb_init_cartesian_lism": (C.c_int32, [C.POINTER(C.c_void_p), C.POINTER(CartDesc), C.POINTER(LismIC)]),
     "setb_cart_fill_lism": (C.c_int32, [C.POINTER(CartDesc), C.POINTER(LismIC), _dp]),
@@ -248,6 +252,51 @@ def chlld_batch(n_state, normals, q1, q2, w=None, n_disc=0, precision=0):
                                 _p(qqq), _p(sp), fl.ctypes.data_as(_ip))
     _check(rc, "setb_chlld_batch")
     return qqq, sp, fl
+
+
+def chlld_q(n_state, normal, w, qqq1, qqq2, n_disc=None, ydar=None, konvect=None, null_bn=None,
+            p_correct=None):
+    """The reference's chlld_Q signature on the host (Solvers.f90:198-201).  qqq1 / qqq2 are
+    9-vectors (Q last); konvect is None or (left, right) of the second scalar; the logical
+    OPTIONAL arguments are None (absent) or bools.  Returns (qqq[9], dsl, dsp, dsc, kflux) with
+    kflux None when konvect is None."""
+    q1 = np.ascontiguousarray(qqq1, dtype=np.float64)
+    q2 = np.ascontiguousarray(qqq2, dtype=np.float64)
+    if q1.shape != (9,) or q2.shape != (9,):
+        raise ValueError("chlld_q takes 9-component states")
+    out = np.zeros(9)
+    ns = C.c_int32(int(n_state))
+    al, be, ge, wv = (C.c_double(float(normal[0])), C.c_double(float(normal[1])),
+                      C.c_double(float(normal[2])), C.c_double(float(w)))
+    dsl, dsp, dsc = C.c_double(), C.c_double(), C.c_double()
+    opt = lambda v: C.byref(C.c_int32(int(v))) if v is not None else None
+    kv = np.array([konvect[0], konvect[1], 0.0]) if konvect is not None else None
+    rc = lib().setb_chlld_q(C.byref(ns), C.byref(al), C.byref(be), C.byref(ge), C.byref(wv), _p(q1), _p(q2),
+                            C.byref(dsl), C.byref(dsp), C.byref(dsc), _p(out), opt(null_bn), opt(n_disc),
+                            opt(p_correct), _p(kv) if kv is not None else None, opt(ydar))
+    _check(rc, "setb_chlld_q")
+    return out, dsl.value, dsp.value, dsc.value, (None if kv is None else kv[2])
+
+
+def chlld_q_batch(n_state, normals, q1, q2, w=None, n_disc=0, ydar=False, konvect=None):
+    """Batched chlld_Q on the GPU.  normals [n,3], q1/q2 [n,9]; konvect None or [n,2] (left,
+    right).  Returns (qqq [n,9], speeds [n,3], flags [n], kflux [n] or None)."""
+    normals = np.ascontiguousarray(normals, dtype=np.float64)
+    q1 = np.ascontiguousarray(q1, dtype=np.float64)
+    q2 = np.ascontiguousarray(q2, dtype=np.float64)
+    n = q1.shape[0]
+    qqq = np.zeros((n, 9))
+    sp = np.zeros((n, 3))
+    fl = np.zeros(n, dtype=np.int32)
+    kv = None
+    if konvect is not None:
+        kv = np.zeros((n, 3))
+        kv[:, :2] = konvect
+    wp = _p(np.ascontiguousarray(w, dtype=np.float64)) if w is not None else None
+    rc = lib().setb_chlld_q_batch(n, int(n_state), int(n_disc), int(bool(ydar)), _p(normals), wp, _p(q1), _p(q2),
+                                  _p(kv) if kv is not None else None, _p(qqq), _p(sp), fl.ctypes.data_as(_ip))
+    _check(rc, "setb_chlld_q_batch")
+    return qqq, sp, fl, (None if kv is None else kv[:, 2].copy())
 
 
 def step_noalloc(desc: CartDesc, opts: StepOpts, U_ptr: int, var_stride: int, nsteps: int, dt: float,

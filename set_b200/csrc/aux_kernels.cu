@@ -1,5 +1,7 @@
-// aux_kernels.cu -- initial condition, Cell_par <-> conserved conversions, batched chlld.
+// aux_kernels.cu -- initial condition, Cell_par <-> conserved conversions, batched chlld and
+// chlld_Q.
 #include "setb_internal.cuh"
+#include "chlld_q.cuh"
 
 namespace sb {
 namespace {
@@ -75,6 +77,18 @@ __global__ void chlld_batch_kernel(int64_t n, int n_disc, const double* __restri
     }
 }
 
+template <int NSTATE>
+__global__ void chlld_q_batch_kernel(int64_t n, int n_disc, bool ydar, const double* __restrict__ normals,
+                                     const double* __restrict__ w, const double* __restrict__ q1,
+                                     const double* __restrict__ q2, double* __restrict__ konvect,
+                                     double* __restrict__ qqq, double* __restrict__ speeds,
+                                     int32_t* __restrict__ flags) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        chlld_q_general<NSTATE>(normals + 3 * k, w ? w[k] : 0.0, q1 + 9 * k, q2 + 9 * k, n_disc, ydar,
+                                konvect ? konvect + 3 * k : nullptr, qqq + 9 * k, speeds + 3 * k, flags + k);
+    }
+}
+
 int grid_for(long long n, int threads) {
     long long b = (n + threads - 1) / threads;
     if (b < 1) b = 1;
@@ -127,6 +141,22 @@ cudaError_t launch_chlld_batch(int64_t n, int n_state, int n_disc, int precision
         }
     }
 #undef SB_LAUNCH
+    return cudaGetLastError();
+}
+
+cudaError_t launch_chlld_q_batch(int64_t n, int n_state, int n_disc, bool ydar, const double* normals,
+                                 const double* w, const double* q1, const double* q2, double* konvect,
+                                 double* qqq, double* speeds, int32_t* flags, cudaStream_t s) {
+    const int g = grid_for(n, 128);
+#define SB_LAUNCH_Q(NS) \
+    chlld_q_batch_kernel<NS><<<g, 128, 0, s>>>(n, n_disc, ydar, normals, w, q1, q2, konvect, qqq, speeds, flags)
+    switch (n_state) {
+        case 0: SB_LAUNCH_Q(0); break;
+        case 1: SB_LAUNCH_Q(1); break;
+        case 2: SB_LAUNCH_Q(2); break;
+        default: SB_LAUNCH_Q(3); break;
+    }
+#undef SB_LAUNCH_Q
     return cudaGetLastError();
 }
 

@@ -15,6 +15,7 @@
 
 #include "setb200.h"
 #include "setb_internal.cuh"
+#include "chlld_q.cuh"
 
 using namespace sb;
 
@@ -316,6 +317,78 @@ int32_t setb_chlld(const int32_t* n_state, const double* al, const double* be, c
     *dsp = sp[1];
     *dsc = sp[2];
     return (fl & kFlagWave) ? SETB_EWAVES : SETB_OK;
+}
+
+int32_t setb_chlld_q(const int32_t* n_state, const double* al, const double* be, const double* ge, const double* w,
+                     const double qqq1[9], const double qqq2[9], double* dsl, double* dsp, double* dsc, double qqq[9],
+                     const int32_t* null_bn1, const int32_t* n_disc, const int32_t* p_correct_, double* konvect_,
+                     const int32_t* ydar_) {
+    (void)null_bn1;     // overridden to .False. inside chlld_Q (Solvers.f90:267)
+    (void)p_correct_;   // phi_p_correct is set to 1 whatever its value (Solvers.f90:266)
+    if (!n_state || !al || !be || !ge || !w || !qqq1 || !qqq2 || !dsl || !dsp || !dsc || !qqq) return SETB_EINVAL;
+    const int nd = n_disc ? *n_disc : 0;
+    if (*n_state < 0 || *n_state > 3 || nd < 0 || nd > 2) return SETB_EINVAL;
+    const bool ydar = ydar_ && *ydar_ != 0;
+    const double n[3] = {*al, *be, *ge};
+    double sp[3];
+    int32_t fl = 0;
+    switch (*n_state) {
+        case 0: chlld_q_general<0>(n, *w, qqq1, qqq2, nd, ydar, konvect_, qqq, sp, &fl); break;
+        case 1: chlld_q_general<1>(n, *w, qqq1, qqq2, nd, ydar, konvect_, qqq, sp, &fl); break;
+        case 2: chlld_q_general<2>(n, *w, qqq1, qqq2, nd, ydar, konvect_, qqq, sp, &fl); break;
+        default: chlld_q_general<3>(n, *w, qqq1, qqq2, nd, ydar, konvect_, qqq, sp, &fl); break;
+    }
+    *dsl = sp[0];
+    *dsp = sp[1];
+    *dsc = sp[2];
+    return (fl & kFlagWave) ? SETB_EWAVES : SETB_OK;
+}
+
+int32_t setb_chlld_q_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t ydar, const double* normals,
+                           const double* w, const double* q1, const double* q2, double* konvect, double* qqq,
+                           double* speeds, int32_t* flags) {
+    if (n < 0 || n_state < 0 || n_state > 3 || n_disc < 0 || n_disc > 2) return SETB_EINVAL;
+    if (n == 0) return SETB_OK;
+    if (!normals || !q1 || !q2 || !qqq || !speeds || !flags) return SETB_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SETB_ENODEV;
+    const size_t sn = (size_t)n;
+    double *dn = nullptr, *dw = nullptr, *d1 = nullptr, *d2 = nullptr, *dk = nullptr, *dq = nullptr, *ds = nullptr;
+    int32_t* df = nullptr;
+    cudaStream_t s = nullptr;
+    int rc = SETB_OK;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return SETB_ECUDA;
+    if (cudaMalloc(&dn, 3 * sn * 8) || (w && cudaMalloc(&dw, sn * 8)) || cudaMalloc(&d1, 9 * sn * 8) ||
+        cudaMalloc(&d2, 9 * sn * 8) || (konvect && cudaMalloc(&dk, 3 * sn * 8)) || cudaMalloc(&dq, 9 * sn * 8) ||
+        cudaMalloc(&ds, 3 * sn * 8) || cudaMalloc(&df, sn * 4)) {
+        cudaGetLastError();
+        rc = SETB_ENOMEM;
+    }
+    if (rc == SETB_OK) {
+        bool ok = cudaMemcpyAsync(dn, normals, 3 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+                  (!w || cudaMemcpyAsync(dw, w, sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess) &&
+                  cudaMemcpyAsync(d1, q1, 9 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+                  cudaMemcpyAsync(d2, q2, 9 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+                  (!konvect || cudaMemcpyAsync(dk, konvect, 3 * sn * 8, cudaMemcpyHostToDevice, s) == cudaSuccess) &&
+                  launch_chlld_q_batch(n, n_state, n_disc, ydar != 0, dn, dw, d1, d2, dk, dq, ds, df, s) ==
+                      cudaSuccess &&
+                  cudaMemcpyAsync(qqq, dq, 9 * sn * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                  cudaMemcpyAsync(speeds, ds, 3 * sn * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                  cudaMemcpyAsync(flags, df, sn * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+                  (!konvect || cudaMemcpyAsync(konvect, dk, 3 * sn * 8, cudaMemcpyDeviceToHost, s) == cudaSuccess) &&
+                  cudaStreamSynchronize(s) == cudaSuccess;
+        if (!ok) rc = SETB_ECUDA;
+    }
+    cudaFree(dn);
+    cudaFree(dw);
+    cudaFree(d1);
+    cudaFree(d2);
+    cudaFree(dk);
+    cudaFree(dq);
+    cudaFree(ds);
+    cudaFree(df);
+    cudaStreamDestroy(s);
+    return rc;
 }
 
 int32_t setb_chlld_batch(int64_t n, int32_t n_state, int32_t n_disc, int32_t precision, const double* normals,

@@ -216,18 +216,14 @@ SB_HD void lism_cell(const GridGeom& g, const double* lism, uint64_t seed, doubl
     cons_from_prim_exact(q, U);
 }
 
-// General-normal chlld for a batch of faces: the lab states are rotated into an orthonormal
-// face frame (the reference's basis construction, Solvers.f90:1236-1273), solved, and the
-// momentum / B fluxes rotated back.
-template <typename T, int NSTATE, bool DELTA = false>
-SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const double* q2d, int n_disc,
-                          double* qqq, double* sp, int32_t* flag) {
+// Tangent basis (e2, e3) of a face with unit normal nrm, from the field averaged over the two
+// sides (the reference's aco construction, Solvers.f90:1236-1273; chlld_Q :323-360).
+SB_HD void face_basis(const double* nrm, const double* q1d, const double* q2d, double* e2, double* e3) {
     const double al = nrm[0], be = nrm[1], ge = nrm[2];
     double bav[3];
     for (int c = 0; c < 3; c++) bav[c] = 0.5 * (q1d[5 + c] + q2d[5 + c]) * kInvSpi4;
     const double bk = bav[0] * al + bav[1] * be + bav[2] * ge;
     double d = (bav[0] * bav[0] + bav[1] * bav[1] + bav[2] * bav[2]) - bk * bk;
-    double e2[3], e3[3];
     if (d > 1.0e-12) {
         d = sqrt(d);
         e2[0] = (bav[0] - bk * al) / d;
@@ -250,6 +246,16 @@ SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const d
         e3[1] = (ai[2] * al - ai[0] * ge) / d;
         e3[2] = (ai[0] * be - ai[1] * al) / d;
     }
+}
+
+// General-normal chlld for a batch of faces: the lab states are rotated into an orthonormal
+// face frame (face_basis), solved, and the momentum / B fluxes rotated back.
+template <typename T, int NSTATE, bool DELTA = false>
+SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const double* q2d, int n_disc,
+                          double* qqq, double* sp, int32_t* flag) {
+    const double al = nrm[0], be = nrm[1], ge = nrm[2];
+    double e2[3], e3[3];
+    face_basis(nrm, q1d, q2d, e2, e3);
     T a[8], b[8], F[8], SL, SR, SM;
     const double* qs[2] = {q1d, q2d};
     T* outs[2] = {a, b};
@@ -350,6 +356,9 @@ cudaError_t launch_chlld_batch(int64_t n, int n_state, int n_disc, int precision
                                const double* normals, const double* w, const double* q1,
                                const double* q2, double* qqq, double* speeds, int32_t* flags,
                                cudaStream_t s);
+cudaError_t launch_chlld_q_batch(int64_t n, int n_state, int n_disc, bool ydar, const double* normals,
+                                 const double* w, const double* q1, const double* q2, double* konvect,
+                                 double* qqq, double* speeds, int32_t* flags, cudaStream_t s);
 int stage_fp64_smem_bytes();
 
 }  // namespace sb
