@@ -245,7 +245,14 @@ typedef struct {
                                    (Source_MK, cuf_kernel.cuf:215-288), the v clamp near the
                                    axis (:783-785) and the Lax flux on near-axis faces
                                    (cuf_solvers.cuf:293-295).  Cell centres need y > 0.          */
-    int32_t reserved;           /* must be 0                                                     */
+    int32_t powell;             /* physics 0 only.  0: off (the reference: Gran_POTOK(9) = 0,
+                                   cuf_solvers.cuf:433).  1: the reference's div-B terms, commented
+                                   out there (cuf_solvers.cuf:433, 529-533, 729-733): face flux
+                                   Gran_POTOK(9) = 0.5 n.(B1 + B2) * square, sks = its owner-signed
+                                   sum over the cell's faces, sources -(B/4pi) sks on the momentum
+                                   and -u sks on B (in the flux sum, before the division by the
+                                   volume), u and B of the stage input.  2: as 1 plus Powell's
+                                   energy source -(u.B/4pi) sks.                                 */
 } setb_fl_params;
 
 /* Replaces Set_CUDA for the reference's grid (cuf_kernel.cuf:351-382). */

@@ -263,7 +263,7 @@ class OrcFaceList(C.Structure):
                 ("r_src", C.c_double), ("rho_src", C.c_double), ("v_src", C.c_double),
                 ("p_over_rho_src", C.c_double), ("r_floor", C.c_double), ("dt_init", C.c_double),
                 ("face_skip_radius", C.c_double), ("cell_freeze_radius", C.c_double),
-                ("hatom", _dp), ("physics", C.c_int32), ("reserved", C.c_int32)]
+                ("hatom", _dp), ("physics", C.c_int32), ("powell", C.c_int32)]
 
 
 def facelist(mesh, params, cell_par=None) -> OrcFaceList:
@@ -271,7 +271,7 @@ def facelist(mesh, params, cell_par=None) -> OrcFaceList:
     parameters (anything with the fields of setb_fl_params); cell_par [N,16] supplies the H-atom
     fluids (columns 9..16) of physics 1.  Keep `mesh` and the returned object's `_keep` alive."""
     m = OrcFaceList()
-    m.physics, m.reserved = int(getattr(params, "physics", 0)), 0
+    m.physics, m.powell = int(getattr(params, "physics", 0)), int(getattr(params, "powell", 0))
     if cell_par is not None:
         h = np.ascontiguousarray(np.asarray(cell_par, dtype=np.float64)[:, 8:16])
         m.hatom = _p(h)

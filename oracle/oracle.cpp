@@ -1375,8 +1375,10 @@ typedef struct {
     double face_skip_radius;    // faces whose first cell has |centre| < this are skipped
     double cell_freeze_radius;  // cells with |centre| < this are not updated
     const double* hatom;        // physics 1: Cell_par columns 9..16 per cell ([N][8]), or null
-    int32_t physics, reserved;  // 0: 3D MHD conservative update; 1: the reference's axisymmetric
+    int32_t physics;            // 0: 3D MHD conservative update; 1: the reference's axisymmetric
                                 // hydro update with charge exchange
+    int32_t powell;             // physics 0: 0 off, 1 the reference's commented div-B terms
+                                // (cuf_solvers.cuf:433, 529-533), 2 plus the energy term
 } orc_facelist;
 
 // SET_Fortran_Cuda_MHD/cuf_kernel.cuf:215-288, Source_MK: charge-exchange momentum (x, y) and
@@ -1498,7 +1500,11 @@ static double fl_face(const orc_facelist* m, const orc_opts* o, const double* P,
     }
     const double sq = m->gran_square[gr];
     for (int v = 0; v < 8; v++) F[v] = pot[v] * sq;   // :431
-    F[8] = 0.0;                                        // :433
+    // :433: 0 live; the commented expression 0.5 * DOT_PRODUCT(Gran_normal, qqq1(6:8) + qqq2(6:8))
+    // * square when the div-B terms are on (qqq1 / qqq2: the states given to chlld)
+    F[8] = 0.0;
+    if (m->powell)
+        F[8] = 0.5 * ((n[0] * (q1[5] + q2[5]) + n[1] * (q1[6] + q2[6])) + n[2] * (q1[7] + q2[7])) * sq;
     return std::min(dt_face_cap, o->cfl * dist / (std::max(std::fabs(dsl), std::fabs(dsp)) + std::fabs(wc)));
 }
 
@@ -1589,13 +1595,26 @@ static void fl_stage(const orc_facelist* m, const orc_opts* o, const double* Uin
                     cons_from_prim(qn, un);
                 }
             } else {
-                double pot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                double pot[8] = {0, 0, 0, 0, 0, 0, 0, 0}, sks = 0.0;
                 for (int f = 0; f < 6; f++) {                                         // :691-703
                     const int32_t j = m->cell_gran[6 * c + f];
                     if (j == 0) continue;
                     const double* Fj = Fl + 9 * (int64_t)(j - 1);
                     const bool owner = m->gran_neighbour[2 * (int64_t)(j - 1)] == (int32_t)(c + 1);
                     for (int v = 0; v < 8; v++) pot[v] = owner ? pot[v] + Fj[v] : pot[v] - Fj[v];
+                    sks = owner ? sks + Fj[8] : sks - Fj[8];
+                }
+                if (m->powell) {
+                    // :529-533 / :729-733 (commented there): w3 carries + (qqq(8)/cpi4) * sks and
+                    // B carries + qqq(2..4) * sks inside the flux sum; the same for every momentum
+                    // component; powell 2 adds the energy term (u.B/cpi4) * sks.  qqq: the stage
+                    // input's primitive state.
+                    const double* q = &P[(size_t)c * 8];
+                    for (int a = 0; a < 3; a++) {
+                        pot[1 + a] += (q[5 + a] / cpi4) * sks;
+                        pot[5 + a] += q[1 + a] * sks;
+                    }
+                    if (m->powell == 2) pot[4] += (((q[1] * q[5] + q[2] * q[6]) + q[3] * q[7]) / cpi4) * sks;
                 }
                 const double vol = m->cell_volume[c];
                 for (int v = 0; v < 8; v++) {

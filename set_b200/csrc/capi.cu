@@ -475,7 +475,8 @@ int32_t setb_init_facelist(setb_handle** out, int32_t n_cell, int32_t n_gran, co
                            const setb_fl_params* params) {
     if (!out || !cell_par || !params || n_cell < 1 || n_gran < 1) return SETB_EINVAL;
     *out = nullptr;
-    if (!(params->dt_init > 0.0) || params->physics < 0 || params->physics > 1 || params->reserved != 0)
+    if (!(params->dt_init > 0.0) || params->physics < 0 || params->physics > 1 ||
+        params->powell < 0 || params->powell > 2 || (params->powell != 0 && params->physics != 0))
         return SETB_EINVAL;
     if (params->physics == 1)   // the axisymmetric update divides by the radius y
         for (int32_t c = 0; c < n_cell; c++)

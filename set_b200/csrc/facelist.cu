@@ -16,9 +16,10 @@
 //     needs no host round trip;
 //   * the face flux array persists between stages: a skipped face keeps its previous flux, as
 //     Gran_POTOK does in the reference.
-// The cell update is the conservative ideal-MHD update of all 8 variables used by the Cartesian
-// path (the reference's live cell kernel is a 2D axisymmetric hydro update; its geometric and
-// charge-exchange sources are not part of this path).
+// Physics 0 is the conservative ideal-MHD update of all 8 variables used by the Cartesian path,
+// optionally with the div-B terms the reference carries commented out (face flux Gran_POTOK(9),
+// sources proportional to its owner-signed sum); physics 1 is the reference's live cell kernel,
+// a 2D axisymmetric hydro update with charge exchange.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -52,6 +53,8 @@ struct FaceListDev {
     GridGeom src{};                  // source-sphere parameters (r_src 0 = none)
     int physics = 0;                 // 0: 3D MHD; 1: the reference's axisymmetric hydro update
     double* hatom = nullptr;         // physics 1: [N][8] H-atom fluids (Cell_par columns 9..16)
+    int powell = 0;                  // physics 0: div-B terms (0 off, 1 momentum + induction, 2 + energy)
+    double* divb = nullptr;          // powell: [G] div-B face flux * area, Gran_POTOK(9) (persistent)
     // locality order: device cell d holds the caller's cell perm[d] (both 0-based)
     std::vector<int32_t> perm;
 };
@@ -282,6 +285,11 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
         double2* f2 = reinterpret_cast<double2*>(m.flux + 8 * gr);
 #pragma unroll
         for (int v = 0; v < 4; v++) f2[v] = make_double2(qqq[2 * v] * sq, qqq[2 * v + 1] * sq);
+        if (m.powell) {   // :433 as commented there: 0.5 * n.(B1 + B2) * square, B of the chlld states
+            const double nb = dadd(dadd(dmul(n[0], dadd(q1[5], q2[5])), dmul(n[1], dadd(q1[6], q2[6]))),
+                                   dmul(n[2], dadd(q1[7], q2[7])));
+            m.divb[gr] = dmul(dmul(0.5, nb), sq);
+        }
         if (WANT_DT) cand = fmin(kDtFaceCap, cfl * dist / fmax(fabs(sp[0]), fabs(sp[1])));
     }
     if (n_recon) atomicAdd(&cnt[0], (unsigned long long)n_recon);
@@ -353,7 +361,7 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
                 atomicAdd(&cnt[1], 1ull);
             }
         } else {
-            double pot[8];
+            double pot[8], sks = 0.0;
 #pragma unroll
             for (int v = 0; v < 8; v++) pot[v] = 0.0;
             for (int f = 0; f < 6; f++) {
@@ -367,6 +375,23 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
                     const double2 d = f2[v];
                     pot[2 * v] = owner ? pot[2 * v] + d.x : pot[2 * v] - d.x;
                     pot[2 * v + 1] = owner ? pot[2 * v + 1] + d.y : pot[2 * v + 1] - d.y;
+                }
+                if (m.powell) sks = owner ? sks + m.divb[jf] : sks - m.divb[jf];
+            }
+            if (m.powell) {
+                // div-B sources inside the flux sum (cuf_solvers.cuf:529-533 / 729-733, commented
+                // there): momentum + (B/4pi) sks, B + u sks, powell 2 energy + (u.B/4pi) sks, with
+                // u and B of the stage input (the primitive pass of this stage)
+                double q[8];
+                load_prim(m.prim, c, q);
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    pot[1 + a] = dadd(pot[1 + a], dmul(q[5 + a] / kCpi4, sks));
+                    pot[5 + a] = dadd(pot[5 + a], dmul(q[1 + a], sks));
+                }
+                if (m.powell == 2) {
+                    const double ub = dadd(dadd(dmul(q[1], q[5]), dmul(q[2], q[6])), dmul(q[3], q[7]));
+                    pot[4] = dadd(pot[4], dmul(ub / kCpi4, sks));
                 }
             }
             const double vol = m.cell_volume[c];
@@ -435,7 +460,8 @@ void launch_face_n(const FaceListDev& m, int order, bool want_dt, double cfl, in
 void fl_destroy(FaceListDev* f) {
     if (!f) return;
     void* ptrs[] = {f->cell_center, f->cell_volume, f->cell_gran, f->cell_flag, f->normal, f->square, f->geo,
-                    f->nb,          f->nbt,         f->type,      f->prim,      f->flux,   f->hatom};
+                    f->nb,          f->nbt,         f->type,      f->prim,      f->flux,   f->hatom,
+                    f->divb};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete f;
@@ -596,6 +622,7 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
     f->src.r_floor = p->r_floor;
     f->perm = cperm;
     f->physics = p->physics;
+    f->powell = p->powell;
     bool ok = upload(&f->cell_center, cell_center.data(), 3 * (size_t)N, s) == cudaSuccess &&
               upload(&f->cell_volume, cell_volume.data(), (size_t)N, s) == cudaSuccess &&
               upload(&f->cell_gran, cell_gran.data(), 6 * (size_t)N, s) == cudaSuccess &&
@@ -610,6 +637,8 @@ int fl_create(FaceListDev** out, int64_t N, int64_t G, const double* cell_center
               cudaMalloc(&f->flux, sizeof(double) * 8 * (size_t)G) == cudaSuccess &&
               (p->physics != 1 || cudaMalloc(&f->hatom, sizeof(double) * 8 * (size_t)N) == cudaSuccess) &&
               cudaMemsetAsync(f->flux, 0, sizeof(double) * 8 * (size_t)G, s) == cudaSuccess &&
+              (p->powell == 0 || (cudaMalloc(&f->divb, sizeof(double) * (size_t)G) == cudaSuccess &&
+                                  cudaMemsetAsync(f->divb, 0, sizeof(double) * (size_t)G, s) == cudaSuccess)) &&
               cudaStreamSynchronize(s) == cudaSuccess;   // host vectors are released on return
     if (!ok) {
         cudaGetLastError();

@@ -21,17 +21,19 @@ class FlParams(C.Structure):
     _fields_ = [("r_src", C.c_double), ("rho_src", C.c_double), ("v_src", C.c_double),
                 ("p_over_rho_src", C.c_double), ("r_floor", C.c_double), ("dt_init", C.c_double),
                 ("face_skip_radius", C.c_double), ("cell_freeze_radius", C.c_double),
-                ("physics", C.c_int32), ("reserved", C.c_int32)]
+                ("physics", C.c_int32), ("powell", C.c_int32)]
 
 
 def fl_params(r_src=0.125, rho_src=50.0, v_src=10.0, p_over_rho_src=0.01, r_floor=0.0, dt_init=2e-9,
-              face_skip_radius=0.0, cell_freeze_radius=0.0, physics=0) -> FlParams:
+              face_skip_radius=0.0, cell_freeze_radius=0.0, physics=0, powell=0) -> FlParams:
     """physics 0: conservative 3D ideal MHD; 1: the reference's axisymmetric hydro cell update
-    with charge exchange against the H-atom fluids of Cell_par columns 9..16."""
+    with charge exchange against the H-atom fluids of Cell_par columns 9..16.  powell (physics 0):
+    0 off, 1 the reference's div-B flux and momentum / induction sources, 2 plus the energy
+    source."""
     p = FlParams()
     p.r_src, p.rho_src, p.v_src, p.p_over_rho_src, p.r_floor = r_src, rho_src, v_src, p_over_rho_src, r_floor
     p.dt_init, p.face_skip_radius, p.cell_freeze_radius = dt_init, face_skip_radius, cell_freeze_radius
-    p.physics, p.reserved = int(physics), 0
+    p.physics, p.powell = int(physics), int(powell)
     return p
 
 

@@ -142,3 +142,93 @@ def test_oracle_source_mk_moves_plasma_towards_the_atoms():
     U = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1).copy()
     O.fl_run(om, O.make_opts(2, 1, 1, 0.4), U, 1)
     assert (U[1] > 0).all()
+
+
+def _nonsolenoidal_cellpar(m, seed):
+    cp = FL.lism_cellpar(m, seed=seed, pert_amp=0.05)
+    rng = np.random.default_rng(seed + 100)
+    cp[:, 5:8] += rng.normal(0.0, 0.3, (m.n_cell, 3))   # random B: div B != 0 in every cell
+    return cp
+
+
+def _sks(m, divb):
+    """Owner-signed sum of the div-B face fluxes over each cell's faces (cuf_solvers.cuf:691-703)."""
+    s = np.zeros(m.n_cell)
+    for c in range(m.n_cell):
+        for j in m.cell_gran[c]:
+            if j == 0:
+                continue
+            s[c] += divb[j - 1] if m.gran_neighbour[j - 1, 0] == c + 1 else -divb[j - 1]
+    return s
+
+
+def test_oracle_divb_face_flux_is_the_commented_expression():
+    """Gran_POTOK(9) with the div-B terms on: 0.5 * n.(B1 + B2) * square of the states given to
+    chlld (cuf_solvers.cuf:433, commented there); a ghost face's second state carries B1."""
+    m = FL.box_facelist((5, 4, 4), stretch=0.4, seed=2, permute_seed=6)
+    cp = _nonsolenoidal_cellpar(m, 3)
+    om = O.facelist(m, FL.fl_params(r_src=0.0, dt_init=1e-4, powell=1))
+    U = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1).copy()
+    _, _, flux = O.fl_run(om, O.make_opts(3, 1, 1, 0.4), U, 1)
+    B = cp[:, 5:8]
+    s1 = m.gran_neighbour[:, 0] - 1
+    s2 = np.where(m.gran_neighbour[:, 1] > 0, m.gran_neighbour[:, 1] - 1, s1)
+    n, bs = m.gran_normal, B[s1] + B[s2]
+    want = 0.5 * ((n[:, 0] * bs[:, 0] + n[:, 1] * bs[:, 1]) + n[:, 2] * bs[:, 2]) * m.gran_square
+    np.testing.assert_array_equal(flux[:, 8], want)
+    # off (the reference's live code): zero
+    _, _, flux0 = O.fl_run(O.facelist(m, FL.fl_params(r_src=0.0, dt_init=1e-4)), O.make_opts(3, 1, 1, 0.4),
+                           O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1).copy(), 1)
+    assert not flux0[:, 8].any()
+
+
+@pytest.mark.parametrize("powell", [1, 2])
+def test_oracle_powell_sources_match_their_definition(powell):
+    """One forward-Euler step: the div-B run differs from the plain one by -dt/V times
+    (0, B/4pi sks, [u.B/4pi sks], u sks); rho (and E without the energy term) bit for bit."""
+    m = FL.box_facelist((6, 5, 4), stretch=0.3, seed=4)
+    cp = _nonsolenoidal_cellpar(m, 5)
+    o = O.make_opts(3, 1, 1, 0.4)
+    U0 = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1)
+    Up, Uq = U0.copy(), U0.copy()
+    dt = 1e-4
+    O.fl_run(O.facelist(m, FL.fl_params(r_src=0.0, dt_init=dt)), o, Up, 1)
+    _, _, flux = O.fl_run(O.facelist(m, FL.fl_params(r_src=0.0, dt_init=dt, powell=powell)), o, Uq, 1)
+    sks = _sks(m, flux[:, 8])
+    assert np.abs(sks).max() > 1e-3
+    u, B = cp[:, 1:4], cp[:, 5:8]
+    src = np.zeros((8, m.n_cell))
+    src[1:4] = (B / (4 * np.pi) * sks[:, None]).T
+    src[5:8] = (u * sks[:, None]).T
+    if powell == 2:
+        src[4] = (u * B).sum(1) / (4 * np.pi) * sks
+    d = Uq - Up
+    want = -dt * src / m.cell_volume
+    scale = np.maximum(np.abs(U0).max(axis=1, keepdims=True), 1e-3)   # w = 0 in the LISM state
+    assert (np.abs(d - want) / scale).max() <= 1e-13
+    np.testing.assert_array_equal(Uq[0], Up[0])
+    if powell == 1:
+        np.testing.assert_array_equal(Uq[4], Up[4])
+
+
+def test_oracle_powell_vanishes_with_a_uniform_field():
+    """A uniform field has no divergence: over one forward-Euler stage (the field is uniform in
+    its input) the div-B terms change nothing beyond rounding; the closed cells' outward area
+    vectors sum to zero."""
+    m = FL.box_facelist((6, 5, 5), stretch=0.5, seed=7)
+    cp = FL.lism_cellpar(m, seed=8, pert_amp=0.05)     # uniform B, perturbed rho and p
+    o = O.make_opts(3, 2, 1, 0.4)
+    U0 = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1)
+    Up, Uq = U0.copy(), U0.copy()
+    O.fl_run(O.facelist(m, FL.fl_params(r_src=0.0, dt_init=1e-3)), o, Up, 1)
+    O.fl_run(O.facelist(m, FL.fl_params(r_src=0.0, dt_init=1e-3, powell=2)), o, Uq, 1)
+    assert (np.abs(Uq - Up) / np.maximum(np.abs(U0).max(axis=1, keepdims=True), 1e-3)).max() <= 1e-12
+
+
+def test_powell_option_is_validated_on_the_host():
+    m = FL.box_facelist((4, 3, 2), lo=(-1.0, 0.1, -0.1), hi=(1.0, 1.0, 0.1), seed=1)
+    cp = FL.lism_cellpar(m)
+    for params in (FL.fl_params(powell=3), FL.fl_params(powell=-1), FL.fl_params(physics=1, powell=1)):
+        with pytest.raises(S.SetbError) as e:
+            FL.FaceListSolver(m, cp, params)
+        assert e.value.code == 1

@@ -138,3 +138,29 @@ def test_axisymmetric_charge_exchange_matches_oracle(scheme):
         assert dg.n_negdens == dgo.n_negdens == 0
     # the axisymmetric update keeps w and B at zero; charge exchange moves momentum
     assert np.abs(Ug[3]).max() == 0.0 and np.abs(Ug[5:]).max() == 0.0
+
+
+@pytest.mark.parametrize("powell,order,scheme", [(1, 2, 2), (2, 2, 2), (2, 1, 1)])
+def test_facelist_divb_terms_match_oracle(powell, order, scheme):
+    """The div-B option (face flux Gran_POTOK(9) and the sks sources, commented out in the
+    reference at cuf_solvers.cuf:433, 529-533, 729-733) on a field with nonzero divergence."""
+    m = FL.box_facelist((12, 10, 9), stretch=0.5, seed=1, permute_seed=5)
+    params = FL.fl_params(r_src=0.3, rho_src=20.0, v_src=3.0, dt_init=1e-3, powell=powell)
+    cp = FL.lism_cellpar(m, seed=3, pert_amp=0.05, params=params)
+    rng = np.random.default_rng(9)
+    cp[:, 5:8] += rng.normal(0.0, 0.1, (m.n_cell, 3))
+    opts_o = O.make_opts(3, order, scheme, 0.4)
+    opts_g = S.step_opts(n_state=3, order=order, scheme=scheme, cfl=0.4)
+    Uo, cko, _ = oracle_run(m, params, cp, opts_o, 1)
+    Ug, tg, _ = gpu_run(m, params, cp, opts_g, 1)
+    rel = np.abs(Ug - Uo) / (np.abs(Uo).max(axis=1, keepdims=True) + 1e-300)
+    assert rel.max() <= 1e-12, rel.max()
+    # the terms act: the plain run differs by far more than the tolerance
+    Up, _, _ = gpu_run(m, FL.fl_params(r_src=0.3, rho_src=20.0, v_src=3.0, dt_init=1e-3), cp, opts_g, 1)
+    assert (np.abs(Up - Uo) / (np.abs(Uo).max(axis=1, keepdims=True) + 1e-300)).max() > 1e-8
+    Uo, cko, dgo = oracle_run(m, params, cp, opts_o, 20)
+    Ug, tg, dg = gpu_run(m, params, cp, opts_g, 20)
+    l1 = np.abs(Ug - Uo).sum(1) / (np.abs(Uo).sum(1) + 1e-300)
+    assert l1.max() <= 1e-10, l1
+    assert abs(tg - cko.time_all) <= 1e-12 * cko.time_all
+    assert dg.n_negdens == dgo.n_negdens == 0
