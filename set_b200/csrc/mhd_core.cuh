@@ -89,6 +89,65 @@ SB_HD float sb_rsqrt(float x) {
     return 1.0f / std::sqrt(x);
 #endif
 }
+// The Riemann solver's special functions.  FP32: the approximations above.  FP64 on the device:
+// the FP64 approximate instructions (relative error ~1e-6, measured) refined by Newton-Raphson
+// iteration -- two steps y <- y + y (1 - x y) for 1/x, two steps y <- y + (y/2)(1 - x y^2) for
+// 1/sqrt(x) -- and sqrt(x) as x y after one such step, corrected by one step of Heron's method
+// s <- s + (y/2)(x - s^2).  Measured on 2^20 inputs spanning 1e-9..1e9: 1/x and sqrt(x) correctly
+// rounded, 1/sqrt(x) within 1 ulp.  These dependent fused multiply-adds are a shorter chain than
+// the correctly rounded library forms, which the FP64 flux's latency-bound schedule rewards; the
+// state conversions and the mixed form keep the library forms (there the Newton forms measured
+// slower).  On the host all three are the IEEE operations.
+SB_HD double rs_rcp(double x) {
+#if defined(__CUDA_ARCH__)
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    y = fma(y, fma(-x, y, 1.0), y);
+    return fma(y, fma(-x, y, 1.0), y);
+#else
+    return 1.0 / x;
+#endif
+}
+SB_HD double rs_rsqrt(double x) {
+#if defined(__CUDA_ARCH__)
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
+    return fma(0.5 * y, fma(-x * y, y, 1.0), y);
+#else
+    return 1.0 / std::sqrt(x);
+#endif
+}
+SB_HD double rs_sqrt(double x) {
+#if defined(__CUDA_ARCH__)
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
+    const double s = x * y;
+    const double r = fma(0.5 * y, fma(-s, s, x), s);
+    return x == 0.0 ? x : r;   // the seed of 0 is infinite
+#else
+    return std::sqrt(x);
+#endif
+}
+SB_HD float rs_rcp(float x) { return sb_rcp(x); }
+SB_HD float rs_rsqrt(float x) { return sb_rsqrt(x); }
+SB_HD float rs_sqrt(float x) { return sb_sqrt(x); }
+// NR = false selects the library forms (riemann's FP64 recompute inside the mixed and delta
+// kernels, whose schedules measured faster that way).
+template <bool NR, typename T> SB_HD T fr_rcp(T x) {
+    if constexpr (NR) return rs_rcp(x);
+    else return sb_rcp(x);
+}
+template <bool NR, typename T> SB_HD T fr_rsqrt(T x) {
+    if constexpr (NR) return rs_rsqrt(x);
+    else return sb_rsqrt(x);
+}
+template <bool NR, typename T> SB_HD T fr_sqrt(T x) {
+    if constexpr (NR) return rs_sqrt(x);
+    else return sb_sqrt(x);
+}
+
 template <typename T> SB_HD T sb_abs(T x) { return x < T(0) ? -x : x; }
 template <typename T> SB_HD T sb_min(T a, T b) { return b < a ? b : a; }
 template <typename T> SB_HD T sb_max(T a, T b) { return a < b ? b : a; }
@@ -133,7 +192,7 @@ SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
 // SL, SR, SM (chlld's dsl, dsp, dsc).  wv is the face speed (used only when MOVING).
 // Returns a bit set: kFlagWave when no wave-fan region matched (the reference STOPs),
 // kFlagStar (CHECK_STAR only) when the selected state has rho <= 0 or p <= 0 or F is not finite.
-template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR>
+template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR, bool NR = true>
 SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& SRo, T& SMo) {
     const T ispi4 = T(kInvSpi4);
     const T ga = T(kGamma);
@@ -152,18 +211,18 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     // a = bn/sqrt(r); squaring gives the same speed as
     // cf^2 = (c^2 + b2/r + sqrt((c^2 + b2/r)^2 - 4 c^2 bn^2/r))/2, which needs two square roots
     // per side instead of three plus a reciprocal square root.
-    const T ir1 = sb_rcp(r1), ir2 = sb_rcp(r2);
+    const T ir1 = fr_rcp<NR>(r1), ir2 = fr_rcp<NR>(r2);
     const T b2L = (bx1 * bx1 + by1 * by1) + bz1 * bz1;
     const T b21 = b2L * ir1;
     const T c2L = ga * p1 * ir1;
     const T sL = c2L + b21;
-    const T cfL = sb_sqrt(half * (sL + sb_sqrt(sb_pos(sL * sL - T(4) * c2L * (bx1 * bx1 * ir1)))));
+    const T cfL = fr_sqrt<NR>(half * (sL + fr_sqrt<NR>(sb_pos(sL * sL - T(4) * c2L * (bx1 * bx1 * ir1)))));
     const T ptL = p1 + half * b2L;
     const T b2R = (bx2 * bx2 + by2 * by2) + bz2 * bz2;
     const T b22 = b2R * ir2;
     const T c2R = ga * p2 * ir2;
     const T sR = c2R + b22;
-    const T cfR = sb_sqrt(half * (sR + sb_sqrt(sb_pos(sR * sR - T(4) * c2R * (bx2 * bx2 * ir2)))));
+    const T cfR = fr_sqrt<NR>(half * (sR + fr_sqrt<NR>(sb_pos(sR * sR - T(4) * c2R * (bx2 * bx2 * ir2)))));
     const T ptR = p2 + half * b2R;
 
     // wave-speed estimates, :1308-1330
@@ -171,11 +230,11 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     T SR = sb_max(u1 + cfL, u2 + cfR);
     T cfC = T(0), vC1 = T(0);
     if (n_disc != 0 || NSTATE == 0) {
-        const T aC = half * (bx1 * sb_rsqrt(r1) + bx2 * sb_rsqrt(r2));
+        const T aC = half * (bx1 * fr_rsqrt<NR>(r1) + bx2 * fr_rsqrt<NR>(r2));
         const T b2o = half * (b22 + b21);
-        const T cC = sb_sqrt(ga * (half * (p2 + p1)) * sb_rcp(half * (r2 + r1)));
-        cfC = half * (sb_sqrt(sb_pos(b2o + cC * (cC + T(2) * aC))) +
-                      sb_sqrt(sb_pos(b2o + cC * (cC - T(2) * aC))));
+        const T cC = fr_sqrt<NR>(ga * (half * (p2 + p1)) * fr_rcp<NR>(half * (r2 + r1)));
+        cfC = half * (fr_sqrt<NR>(sb_pos(b2o + cC * (cC + T(2) * aC))) +
+                      fr_sqrt<NR>(sb_pos(b2o + cC * (cC - T(2) * aC))));
         vC1 = half * (u1 + u2);
         if (n_disc == 1) {
             SL = sb_min(u1 - cfL, vC1 - cfC);
@@ -188,7 +247,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         }
     }
     const T suR = SR - u2, suL = SL - u1;
-    const T idd = sb_rcp(suR * r2 - suL * r1);
+    const T idd = fr_rcp<NR>(suR * r2 - suL * r1);
     const T SM = (((suR * r2 * u2 - ptR) + ptL) - suL * r1 * u1) * idd;
     SLo = SL;
     SRo = SR;
@@ -200,7 +259,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     }
 
     int flag = 0;
-    const T isrl = sb_rcp(SR - SL);
+    const T isrl = fr_rcp<NR>(SR - SL);
     // HLL average of the normal field, UZ(6) (:1406-1408 with FL(6) = FR(6) = 0)
     const T bn = (SR * bx2 - SL * bx1) * isrl;
 
@@ -235,7 +294,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         if (SL > wv) TL = T(0);
         if (SR < wv) TR = T(0);
         const T a = TR * TL;
-        const T ib = sb_rcp(TR - TL);
+        const T ib = fr_rcp<NR>(TR - TL);
 #pragma unroll
         for (int k = 0; k < 8; k++) F[k] = ((TR * FL[k] - TL * FR[k]) + a * (UR[k] - UL[k])) * ib;
         if (MOVING) {
@@ -254,7 +313,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         // The wave-fan region needs only SL, SR, SM and the star densities, so it is found first
         // and the energy, physical flux and conserved vector (:1368-1404) and the star energy are
         // formed for the selected side alone.
-        const T isrm = sb_rcp(SR - SM), islm = sb_rcp(SL - SM);
+        const T isrm = fr_rcp<NR>(SR - SM), islm = fr_rcp<NR>(SL - SM);
         const T suRm = suR * isrm, suLm = suL * islm;
         const T rzR = r2 * suRm, rzL = r1 * suLm;
         T vzL2, vzL3, vzR2, vzR3, bzL2, bzL3, bzR2, bzR3;
@@ -278,13 +337,13 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             const T uz3 = ((SR * (r2 * w2) - SL * (r1 * w1)) + FL3 - FR3) * isrl;
             const T uz6 = ((SR * by2 - SL * by1) + FL6 - FR6) * isrl;
             const T uz7 = ((SR * bz2 - SL * bz1) + FL7 - FR7) * isrl;
-            sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * sb_rcp(uz0);
+            sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * fr_rcp<NR>(uz0);
             if (sb_abs(bn) < T(kEpsB)) {
                 vzR2 = v2; vzR3 = w2; vzL2 = v1; vzL3 = w1;
                 bzR2 = by2 * suRm; bzR3 = bz2 * suRm;
                 bzL2 = by1 * suLm; bzL3 = bz1 * suLm;
             } else {
-                const T cR = bn * sb_rcp(suR * r2), cL = bn * sb_rcp(suL * r1);
+                const T cR = bn * fr_rcp<NR>(suR * r2), cL = bn * fr_rcp<NR>(suL * r1);
                 vzR2 = v2 + (by2 - uz6) * cR;
                 vzR3 = w2 + (bz2 - uz7) * cR;
                 vzL2 = v1 + (by1 - uz6) * cL;
@@ -302,13 +361,13 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             T tvR = T(0), tbR = T(0), tvL = T(0), tbL = T(0);
             const T ttR = r2 * suR * (SR - SM) - bn2;
             if (!(sb_abs(ttR) <= T(kTtEps))) {
-                const T i = sb_rcp(ttR);
+                const T i = fr_rcp<NR>(ttR);
                 tvR = (SM - u2) * i;
                 tbR = (r2 * suR * suR - bn2) * i;
             }
             const T ttL = r1 * suL * (SL - SM) - bn2;
             if (!(sb_abs(ttL) <= T(kTtEps))) {
-                const T i = sb_rcp(ttL);
+                const T i = fr_rcp<NR>(ttL);
                 tvL = (SM - u1) * i;
                 tbL = (r1 * suL * suL - bn2) * i;
             }
@@ -320,7 +379,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             bzL3 = bz1 * tbL;
             bzR2 = by2 * tbR;
             bzR3 = bz2 * tbR;
-            const T isR = sb_rsqrt(rzR), isL = sb_rsqrt(rzL);   // 1/sqrt(rho*) and sqrt(rho*) = rho*/sqrt(rho*)
+            const T isR = fr_rsqrt<NR>(rzR), isL = fr_rsqrt<NR>(rzL);   // 1/sqrt(rho*) and sqrt(rho*) = rho*/sqrt(rho*)
             rzRs = rzR * isR;
             rzLs = rzL * isL;
             const T abn = sb_abs(bn);
@@ -338,7 +397,7 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
             else if (SL > wv) region = 1;
             else region = 0;
             if (region == 3 || region == 4) {
-                const T irzss = sb_rcp(rzRs + rzLs);
+                const T irzss = fr_rcp<NR>(rzRs + rzLs);
                 const T rzps = rzRs * rzLs;
                 vzz2 = ((rzLs * vzL2 + rzRs * vzR2) + sbn * (bzR2 - bzL2)) * irzss;
                 vzz3 = ((rzLs * vzL3 + rzRs * vzR3) + sbn * (bzR3 - bzL3)) * irzss;

@@ -200,7 +200,7 @@ __device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j
         for (int v = 0; v < 8; v++) f[s][v] = c[s][perm[v]];
     double q1[8], q2[8], G[8], SM;
     reconstruct<double, ORDER>(f[0], f[1], f[2], f[3], q1, q2);
-    const int fl = riemann<double, NSTATE, false, false>(q1, q2, 0.0, A.n_disc, G, *sl, *sr, SM);
+    const int fl = riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, A.n_disc, G, *sl, *sr, SM);
     for (int v = 0; v < 8; v++) F[perm[v]] = G[v];
     return fl;
 }
@@ -233,7 +233,7 @@ template <int NSTATE>
 __device__ __noinline__ int face_fp64_states(const double* q1, const double* q2, int n_disc, double* F, double* sl,
                                              double* sr) {
     double SM;
-    return riemann<double, NSTATE, false, false>(q1, q2, 0.0, n_disc, F, *sl, *sr, SM);
+    return riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, n_disc, F, *sl, *sr, SM);
 }
 
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT, int SK>
