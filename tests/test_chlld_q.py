@@ -192,3 +192,22 @@ def test_host_chlld_q_rejects_bad_arguments():
         assert e.value.code == 1
     with pytest.raises(ValueError):
         S.chlld_q(3, (1.0, 0.0, 0.0), 0.0, q[:8], q[:8])
+
+
+def test_batch_entry_point_checks_arguments_on_the_host():
+    """setb_chlld_q_batch validates its options before touching a device; an empty batch is a
+    no-op; without a GPU a valid batch reports ENODEV (8), never a CPU result."""
+    import ctypes as C
+    from tests.conftest import has_gpu
+    L = S.lib()
+    q = np.zeros((1, 9))
+    nr = np.array([[1.0, 0.0, 0.0]])
+    out, sp, fl = np.zeros((1, 9)), np.zeros((1, 3)), np.zeros(1, dtype=np.int32)
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    args = lambda n, ns, nd: (n, ns, nd, 0, P(nr), None, P(q), P(q), None, P(out), P(sp),
+                              fl.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert L.setb_chlld_q_batch(*args(0, 3, 0)) == 0
+    for bad in ((1, 4, 0), (1, 3, 3), (-1, 3, 0)):
+        assert L.setb_chlld_q_batch(*args(*bad)) == 1
+    if not has_gpu():
+        assert L.setb_chlld_q_batch(*args(1, 3, 0)) == 8
