@@ -185,7 +185,7 @@ int rebuild(setb_batch* b) {
         Slot& sl = b->slots[s];
         GridGeom g = sl.g;
         g.lz = std::min(b->lz, g.nz);
-        const int ty = tile_shape(b->precision, 1).ty;
+        const int ty = tile_shape(b->precision, kBatchKind).ty;
         const int ntx = (g.nx + kTileX - 1) / kTileX, nty = (g.ny + ty - 1) / ty, ntz = (g.nz + g.lz - 1) / g.lz;
         for (int bz = 0; bz < ntz; bz++)
             for (int by = 0; by < nty; by++)
@@ -381,7 +381,7 @@ int32_t setb_batch_add(setb_batch* b, const setb_cart_desc* d, const setb_lism_i
     sl.st = reinterpret_cast<DevStatus*>(p + 256);
     sl.tmap = reinterpret_cast<CUtensorMap*>(p + 512);
     CUtensorMap tm[2] = {};
-    const int ty = tile_shape(b->precision, 1).ty;
+    const int ty = tile_shape(b->precision, kBatchKind).ty;
     if (encode_state_tmap(sl.g, sl.U, ty, &tm[0]) != SETB_OK || encode_state_tmap(sl.g, sl.W, ty, &tm[1]) != SETB_OK) {
         sl.tmap = nullptr;   // plain loads for this solve
     }

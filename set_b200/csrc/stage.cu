@@ -565,7 +565,7 @@ __global__ void __launch_bounds__(Tile<P, KIND>::NT, Tile<P, KIND>::MINB) stage_
 // tile's solve selects the arguments (copied to shared memory) and the Riemann solver.  The
 // items of one solve are counted by its own clock, so every solve keeps its own lagged dt.
 template <int P, int ORDER, int KIND, bool WANT_DT>
-__global__ void __launch_bounds__(Tile<P, 1>::NT, Tile<P, 1>::MINB) batch_stage_kernel(const BatchArgs B) {
+__global__ void __launch_bounds__(Tile<P, kBatchKind>::NT, Tile<P, kBatchKind>::MINB) batch_stage_kernel(const BatchArgs B) {
     __shared__ __align__(16) StageArgs As;
     __shared__ int4 it;
     __shared__ __align__(8) unsigned long long bar;
@@ -583,12 +583,12 @@ __global__ void __launch_bounds__(Tile<P, 1>::NT, Tile<P, 1>::MINB) batch_stage_
         if (w.x < 0) break;
         const unsigned long long* src = reinterpret_cast<const unsigned long long*>(B.inst + w.x);
         unsigned long long* dst = reinterpret_cast<unsigned long long*>(&As);
-        for (int q = threadIdx.x; q < WORDS; q += Tile<P, 1>::NT) dst[q] = src[q];
+        for (int q = threadIdx.x; q < WORDS; q += Tile<P, kBatchKind>::NT) dst[q] = src[q];
         __syncthreads();
         if (As.n_state == 3)
-            run_tile<P, 3, ORDER, KIND, WANT_DT, 1>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
+            run_tile<P, 3, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
         else
-            run_tile<P, 2, ORDER, KIND, WANT_DT, 1>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
+            run_tile<P, 2, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
     }
 }
 
@@ -639,7 +639,7 @@ cudaError_t launch_p(const StageArgs& a, int n_state, int order, int kind, bool 
 template <int P, int KIND, bool WANT_DT>
 cudaError_t batch_attr() {
     return cudaFuncSetAttribute(batch_stage_kernel<P, 2, KIND, WANT_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem_bytes<P, 1>());
+                                smem_bytes<P, kBatchKind>());
 }
 
 }  // namespace
@@ -658,13 +658,13 @@ cudaError_t prepare_batch_kernels(int precision) {
     return batch_attr<0, 1, false>();
 }
 
-int batch_ctas_per_sm(int precision) { return tile_shape(precision, 1).ctas_per_sm; }
+int batch_ctas_per_sm(int precision) { return tile_shape(precision, kBatchKind).ctas_per_sm; }
 
 template <int P>
 void launch_batch_p(const BatchArgs& b, int kind, bool want_dt, int grid, cudaStream_t s) {
-    constexpr int NT = Tile<P, 1>::NT;
-    if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P, 1>(), s>>>(b);
-    else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P, 1>(), s>>>(b);
+    constexpr int NT = Tile<P, kBatchKind>::NT;
+    if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P, kBatchKind>(), s>>>(b);
+    else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P, kBatchKind>(), s>>>(b);
 }
 
 cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
