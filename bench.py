@@ -38,9 +38,9 @@ BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
 BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
 BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
 # DRAM bytes (read + write) per cell of one plain stage-2 launch, from the ncu capture at 160^3
-# summarised in profiles/stage_plain_hlld_160cube.md (773.98 MB / 4.096 M cells); traffic grows
+# summarised in profiles/stage_plain_hlld_160cube.md (774.07 MB / 4.096 M cells); traffic grows
 # with the cell count, so the full-size launch's traffic is this figure times its cells.
-TRAFFIC_STAGE2_PER_CELL = 773.975296e6 / 160 ** 3
+TRAFFIC_STAGE2_PER_CELL = 774.065152e6 / 160 ** 3
 
 
 def peaks():
