@@ -217,6 +217,77 @@ def run_mixed_only(args):
                       "cell_updates_per_s": n ** 3 * T * args.steps / (sum(ms) / 1e3)}), flush=True)
 
 
+def run_slab(args, world, rank, local):
+    """One grid of n x n x (n * ranks) cells split along z, one n^3 slab per rank, ghost planes
+    exchanged over NCCL each stage and the dt minimum all-reduced each step (weak scaling)."""
+    import numpy as np
+    import torch
+    import set_b200 as S
+    from set_b200 import slab as SL
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n, T = args.n, args.tsteps
+    nz = n * world
+    desc = S.cart_desc((n, n, nz))
+    k0, nl = SL.split_z(nz, world)[rank]
+    rng = np.random.default_rng(2 + rank)   # this rank's planes only (the whole grid needs not fit a host)
+    cp = np.zeros((n * n * nl, 16))
+    cp[:, :8] = S.lism_prim()
+    cp[:, 0] *= 1.0 + 1e-3 * rng.uniform(-1.0, 1.0, n * n * nl)
+    cp[:, 4] *= 1.0 + 1e-3 * rng.uniform(-1.0, 1.0, n * n * nl)
+    slab, ic = SL.SlabSolver(desc, k0, nl, cp), SL.SlabSolver(desc, k0, nl, cp)
+    run = SL.SlabRun(slab, rank, world)
+    opts = S.step_opts(n_state=3, order=2, scheme=2, cfl=0.4)
+    stream = torch.cuda.ExternalStream(slab.stream())
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        slab.copy_from(ic)
+        run.step(T, opts)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            slab.copy_from(ic)
+            run.step(T, opts)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    diag = slab.status()
+    cells = n * n * nz
+    if rank == 0:
+        line = {"metric": "mhd_cell_updates_per_s", "value": cells * T * args.steps / (ms / 1e3),
+                "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (LISM + solar-wind source, seeded)",
+                "config": {"workload": f"one grid split along z: {n}x{n}x{nz}, {n}^3 per GPU, HLLD + minmod + "
+                                       f"Heun RK2, {T} time steps per bench step",
+                           "grid": [n, n, nz], "time_steps_per_step": T, "parallelism": f"slab{world}",
+                           "exchange": "2 ghost planes x 8 variables per neighbour and stage, dt min per step"},
+                "clocks": clk.summary(), "gpu_launches": 2 * T * args.steps,
+                "diag": {"time_all": diag.time_all, "n_negdens": diag.n_negdens}}
+        print(json.dumps(line), flush=True)
+    slab.close()
+    ic.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -439,12 +510,16 @@ def main():
     ap.add_argument("--facelist-n", type=int, default=128, help="face-list leg on an n^3 box (0 = off)")
     ap.add_argument("--serve-max-edge", type=int, default=96)
     ap.add_argument("--serve-max-steps", type=int, default=600)
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="N > 1: independent replicas (default) or one grid split along z across the ranks")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)
     elif args.mixed_only:
         run_mixed_only(args)
+    elif args.decomp == "slab":
+        run_slab(args, world, rank, local)
     elif args.c3 > 0:
         import set_b200  # noqa: F401  (fails loudly without the CUDA library)
         from set_b200 import workloads as WL

@@ -203,6 +203,37 @@ SETB_API int32_t setb_status(setb_handle* h, setb_diag* out);
 /* The CUDA stream the handle launches on (as a void* cudaStream_t). */
 SETB_API int32_t setb_stream(setb_handle* h, void** stream);
 
+/* ------------------------------------------------------------------ z slabs (one grid on many GPUs)
+ * The Cartesian grid d split along z, one slab per rank: the reference runs one grid on one GPU
+ * (cuf_kernel.cuf:780-925); this is the multi-GPU form of the same step.  A slab handle owns
+ * planes [k0, k0 + nz_local) of d (global sizes, nz_local >= 2) and holds two ghost planes below
+ * and above them: buffer planes 0, 1 | owned 2 .. nz_local+1 | nz_local+2, nz_local+3.  One time
+ * step is driven stage by stage on the handle's stream:
+ *   1. fill the ghost planes of the stage-1 input (setb_slab_view(h, 1, ...)) from the
+ *      neighbours' owned edge planes; setb_slab_stage(h, 1, o);
+ *   2. (Heun) fill the ghost planes of the stage-2 input (setb_slab_view(h, 2, ...));
+ *      setb_slab_stage(h, 2, o);
+ *   3. replace the next step's dt (setb_slab_dt) by its minimum over all slabs.
+ * Ghost planes beyond the grid's z ends are filled by setb_slab_stage itself (copies of the end
+ * plane, the zero-gradient boundary).  With those exchanges the slabs reproduce the single-grid
+ * setb_step bit for bit.  setb_get_state / setb_set_state / setb_get_conserved / setb_status /
+ * setb_destroy work on a slab handle (state transfers cover the owned planes; the first bad cell
+ * is a whole-grid index); setb_step refuses one (SETB_EINVAL).  Diagnostic counters count the two
+ * faces on a slab boundary in both slabs. */
+SETB_API int32_t setb_init_slab(setb_handle** h, const setb_cart_desc* d, int32_t k0, int32_t nz_local,
+                                const double* cell_par /* 16 x (nx*ny*nz_local), owned planes */);
+/* Enqueues stage 1 (Euler step or Heun stage 1, with the dt candidate) or stage 2 (Heun stage 2,
+ * rolls the clock) on the handle's stream; Euler steps are stage 1 alone. */
+SETB_API int32_t setb_slab_stage(setb_handle* h, int32_t stage, const setb_step_opts* o);
+/* The device buffer a stage reads (conserved SoA: variable v, buffer plane k, row j, column i at
+ * base[v*var_stride + k*plane_stride + j*row_pitch + i]; row_pitch as setb_state_view) and its
+ * plane count nz_local + 4.  The buffers swap roles after an Euler step. */
+SETB_API int32_t setb_slab_view(setb_handle* h, int32_t stage, double** base, int64_t* var_stride,
+                                int64_t* plane_stride, int32_t* nz_buffer);
+/* Device address of the dt the next step uses (one double), for a minimum over the slabs after
+ * each step (e.g. an in-place NCCL all-reduce with op min on the handle's stream). */
+SETB_API int32_t setb_slab_dt(setb_handle* h, double** dt_next);
+
 SETB_API int32_t setb_destroy(setb_handle* h);
 
 /* ------------------------------------------------------------------ face-list grids

@@ -104,6 +104,11 @@ _SIGS = {
     "setb_copy_state": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "setb_status": (C.c_int32, [C.c_void_p, C.POINTER(Diag)]),
     "setb_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "setb_init_slab": (C.c_int32, [C.POINTER(C.c_void_p), C.POINTER(CartDesc), C.c_int32, C.c_int32, _dp]),
+    "setb_slab_stage": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(StepOpts)]),
+    "setb_slab_view": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(_dp), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_int64), _ip]),
+    "setb_slab_dt": (C.c_int32, [C.c_void_p, C.POINTER(_dp)]),
     "setb_destroy": (C.c_int32, [C.c_void_p]),
     "setb_step_noalloc": (C.c_int32, [C.POINTER(CartDesc), C.POINTER(StepOpts), C.c_void_p, C.c_int64, C.c_int32,
                                       _dp, _dp, C.POINTER(Diag), C.c_void_p]),

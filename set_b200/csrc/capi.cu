@@ -108,11 +108,12 @@ int choose_lz(const GridGeom& g, int sm_count, int precision, int kind) {
     const TileShape ts = tile_shape(precision, kind);
     const long long cols = (long long)((g.nx + kTileX - 1) / kTileX) * ((g.ny + ts.ty - 1) / ts.ty);
     const long long slots = (long long)sm_count * std::max(ts.ctas_per_sm, 1);
+    const int nz = plane_end(g) - plane_begin(g);   // planes the stage kernels update
     double best = 1e300;
-    int best_lz = g.nz;
-    for (int c = 1; c <= std::max(1, g.nz / 8); c++) {
-        const int lz = (g.nz + c - 1) / c;
-        const long long ctas = cols * ((g.nz + lz - 1) / lz);
+    int best_lz = nz;
+    for (int c = 1; c <= std::max(1, nz / 8); c++) {
+        const int lz = (nz + c - 1) / c;
+        const long long ctas = cols * ((nz + lz - 1) / lz);
         const long long waves = (ctas + slots - 1) / slots;
         const double cost = (double)waves * (lz + 1.5);
         if (cost < best - 1e-9) {
@@ -181,7 +182,8 @@ void destroy_impl(setb_handle* h) {
     delete h;
 }
 
-int create_impl(setb_handle** out, const setb_cart_desc* d) {
+// geo: the handle's geometry when it is not the whole grid of d (a z slab)
+int create_impl(setb_handle** out, const setb_cart_desc* d, const GridGeom* geo = nullptr) {
     if (!out) return SETB_EINVAL;
     *out = nullptr;
     int rc = validate_desc(d);
@@ -192,7 +194,7 @@ int create_impl(setb_handle** out, const setb_cart_desc* d) {
     if (!h) return SETB_ENOMEM;
     cudaGetDevice(&h->device);
     h->desc = *d;
-    h->g = make_geom(d);
+    h->g = geo ? *geo : make_geom(d);
     cudaDeviceProp prop{};
     if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess) {
         delete h;
@@ -252,6 +254,15 @@ int upload_cellpar(setb_handle* h, const double* cell_par) {
     h->comp_clean = false;
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
     double* stage = h->buf[1 - h->cur];
+    if (h->g.kb) {   // z slab: the owned planes only; the ghost planes start as zeros
+        const size_t plane = (size_t)h->g.nx * h->g.ny;
+        const size_t own = plane * (size_t)(plane_end(h->g) - plane_begin(h->g));
+        SB_TRY(cudaMemsetAsync(stage, 0, sizeof(double) * 8 * N, h->stream));
+        SB_TRY(cudaMemcpy2DAsync(stage + 8 * plane * (size_t)h->g.kb, 8 * sizeof(double), cell_par, 16 * sizeof(double),
+                                 8 * sizeof(double), own, cudaMemcpyHostToDevice, h->stream));
+        SB_TRY(launch_prim_to_cons(h->g, stage, h->buf[h->cur], h->stream));
+        return SETB_OK;
+    }
     if (const int32_t* perm = fl_perm(h->fl)) {
         const int rc = fl_set_hatom(h->fl, cell_par, h->stream);
         if (rc) return rc;
@@ -563,13 +574,9 @@ int enqueue_fl_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cu
     return SETB_OK;
 }
 
-int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaEvent_t* ev) {
-    if (h->fl) return enqueue_fl_steps(h, nsteps, o, ev);
-    StageArgs a{};
-    a.g = h->g;
-    const int P = o->precision;
-    const int lz0 = choose_lz(h->g, h->sm_count, P, 0), lz1 = choose_lz(h->g, h->sm_count, P, 1);
-    float* comp = nullptr;
+// The mixed form's FP32 compensation: allocated on first use, zeroed when stale.
+int prepare_comp(setb_handle* h, int P, float** comp) {
+    *comp = nullptr;
     if (P != 0) {
         if (!h->comp) {
             if (cudaMalloc(&h->comp, sizeof(float) * 8 * (size_t)h->g.vs) != cudaSuccess) {
@@ -582,10 +589,21 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
             SB_TRY(cudaMemsetAsync(h->comp, 0, sizeof(float) * 8 * (size_t)h->g.vs, h->stream));
             h->comp_clean = true;
         }
-        comp = h->comp;
+        *comp = h->comp;
     } else {
         h->comp_clean = false;   // plain steps leave the compensation stale
     }
+    return SETB_OK;
+}
+
+int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaEvent_t* ev) {
+    if (h->fl) return enqueue_fl_steps(h, nsteps, o, ev);
+    StageArgs a{};
+    a.g = h->g;
+    const int P = o->precision;
+    const int lz0 = choose_lz(h->g, h->sm_count, P, 0), lz1 = choose_lz(h->g, h->sm_count, P, 1);
+    float* comp = nullptr;
+    if (const int rc = prepare_comp(h, P, &comp)) return rc;
     a.clk = h->clk;
     a.st = h->st;
     a.cfl = o->cfl;
@@ -637,7 +655,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
 }  // namespace
 
 int32_t setb_step(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all) {
-    if (!h || nsteps < 0) return SETB_EINVAL;
+    if (!h || nsteps < 0 || h->g.kb) return SETB_EINVAL;   // a z slab steps stage by stage
     int rc = validate_opts(o);
     if (rc) return rc;
     cudaSetDevice(h->device);
@@ -654,7 +672,7 @@ int32_t setb_step(setb_handle* h, int32_t nsteps, const setb_step_opts* o, doubl
 
 int32_t setb_step_profiled(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all,
                            double kernel_ms[2], int32_t launches[2]) {
-    if (!h || nsteps < 0 || !kernel_ms || !launches) return SETB_EINVAL;
+    if (!h || nsteps < 0 || !kernel_ms || !launches || h->g.kb) return SETB_EINVAL;
     int rc = validate_opts(o);
     if (rc) return rc;
     cudaSetDevice(h->device);
@@ -708,8 +726,10 @@ int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_all) {
         SB_TRY(cudaStreamSynchronize(h->stream));
         for (size_t d = 0; d < N; d++) std::memcpy(cell_par + 16 * (size_t)perm[d], &tmp[8 * d], 8 * sizeof(double));
     } else {
-        SB_TRY(cudaMemcpy2DAsync(cell_par, 16 * sizeof(double), stage, 8 * sizeof(double), 8 * sizeof(double), N,
-                                 cudaMemcpyDeviceToHost, h->stream));
+        const size_t plane = (size_t)h->g.nx * h->g.ny;   // a z slab returns its owned planes
+        const size_t own = plane * (size_t)(plane_end(h->g) - plane_begin(h->g));
+        SB_TRY(cudaMemcpy2DAsync(cell_par, 16 * sizeof(double), stage + 8 * plane * (size_t)h->g.kb,
+                                 8 * sizeof(double), 8 * sizeof(double), own, cudaMemcpyDeviceToHost, h->stream));
     }
     int rc = download_clock(h);
     if (rc) return rc;
@@ -754,14 +774,15 @@ int32_t setb_state_view(setb_handle* h, double** base, int64_t* var_stride, int6
 int32_t setb_get_conserved(setb_handle* h, double* U) {
     if (!h || !U) return SETB_EINVAL;
     cudaSetDevice(h->device);
-    const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
+    const int nown = plane_end(h->g) - plane_begin(h->g);   // a z slab returns its owned planes
+    const size_t N = (size_t)h->g.nx * h->g.ny * nown;
     const int32_t* perm = fl_perm(h->fl);
     std::vector<double> tmp(perm ? 8 * N : 0);
     double* dst = perm ? tmp.data() : U;
     for (int v = 0; v < 8; v++)
-        SB_TRY(cudaMemcpy2DAsync(dst + v * N, h->g.nx * sizeof(double), h->buf[h->cur] + v * h->g.vs,
-                                 h->g.px * sizeof(double), h->g.nx * sizeof(double), (size_t)h->g.ny * h->g.nz,
-                                 cudaMemcpyDeviceToHost, h->stream));
+        SB_TRY(cudaMemcpy2DAsync(dst + v * N, h->g.nx * sizeof(double),
+                                 h->buf[h->cur] + v * h->g.vs + (long long)h->g.kb * h->g.ps, h->g.px * sizeof(double),
+                                 h->g.nx * sizeof(double), (size_t)h->g.ny * nown, cudaMemcpyDeviceToHost, h->stream));
     SB_TRY(cudaStreamSynchronize(h->stream));
     if (perm)
         for (int v = 0; v < 8; v++)
@@ -793,6 +814,103 @@ int32_t setb_status(setb_handle* h, setb_diag* out) {
 int32_t setb_stream(setb_handle* h, void** stream) {
     if (!h || !stream) return SETB_EINVAL;
     *stream = (void*)h->stream;
+    return SETB_OK;
+}
+
+// ------------------------------------------------------------------ z slabs
+int32_t setb_init_slab(setb_handle** h, const setb_cart_desc* d, int32_t k0, int32_t nz_local,
+                       const double* cell_par) {
+    if (!h) return SETB_EINVAL;
+    *h = nullptr;
+    int rc = validate_desc(d);
+    if (rc) return rc;
+    if (!cell_par || nz_local < 2 || k0 < 0 || (long long)k0 + nz_local > d->nz) return SETB_EINVAL;
+    GridGeom g = make_geom(d);   // spacing and face areas of the whole grid
+    g.nz = nz_local + 2 * kSlabGhost;
+    set_device_strides(g);
+    g.kb = kSlabGhost;
+    g.ke = nz_local + kSlabGhost;
+    g.koff = k0 - kSlabGhost;
+    g.lz = g.ke - g.kb;
+    rc = create_impl(h, d, &g);
+    if (rc) return rc;
+    setb_handle* s = *h;
+    s->g.lz = choose_lz(s->g, s->sm_count, 0, 0);
+    clock_reset(s, 0.0);
+    rc = upload_cellpar(s, cell_par);
+    if (!rc) rc = upload_clock(s);
+    if (rc) {
+        destroy_impl(s);
+        *h = nullptr;
+    }
+    return rc;
+}
+
+int32_t setb_slab_stage(setb_handle* h, int32_t stage, const setb_step_opts* o) {
+    if (!h || !h->g.kb || (stage != 1 && stage != 2)) return SETB_EINVAL;
+    int rc = validate_opts(o);
+    if (rc) return rc;
+    if (stage == 2 && o->scheme != 2) return SETB_EINVAL;
+    cudaSetDevice(h->device);
+    const GridGeom& g = h->g;
+    const int P = o->precision, kind = stage - 1;
+    const int in = stage == 1 ? h->cur : 1 - h->cur;   // buffer index of the stage input
+    double* U = h->buf[h->cur];
+    double* W = h->buf[1 - h->cur];
+    double* X = h->buf[in];
+    // ghost planes beyond the whole grid's z ends: copies of the end plane (the clamped index of
+    // the single-grid kernel), so a slab reproduces the whole grid bit for bit
+    const size_t pitch = sizeof(double) * (size_t)g.vs, width = sizeof(double) * (size_t)g.ps;
+    if (g.koff + g.kb == 0)
+        for (int p = 0; p < g.kb; p++)
+            SB_TRY(cudaMemcpy2DAsync(X + (long long)p * g.ps, pitch, X + (long long)g.kb * g.ps, pitch, width, 8,
+                                     cudaMemcpyDeviceToDevice, h->stream));
+    if (g.koff + g.ke == h->desc.nz)
+        for (int p = g.ke; p < g.nz; p++)
+            SB_TRY(cudaMemcpy2DAsync(X + (long long)p * g.ps, pitch, X + (long long)(g.ke - 1) * g.ps, pitch, width, 8,
+                                     cudaMemcpyDeviceToDevice, h->stream));
+    float* comp = nullptr;
+    if ((rc = prepare_comp(h, P, &comp))) return rc;
+    const int shape = shape_index(P, kind);
+    StageArgs a{};
+    a.g = g;
+    a.g.lz = choose_lz(g, h->sm_count, P, kind);
+    a.clk = h->clk;
+    a.st = h->st;
+    a.cfl = o->cfl;
+    a.n_disc = o->n_disc;
+    a.Uin = X;
+    a.tm_in = h->tma_ok[shape] ? h->tmap + 2 * in + shape : nullptr;
+    if (stage == 1) {
+        a.Ubase = nullptr;
+        a.Uout = W;
+        a.finalize = o->scheme == 1;
+        a.comp = o->scheme == 1 ? comp : nullptr;
+    } else {
+        a.Ubase = U;
+        a.Uout = U;
+        a.finalize = 1;
+        a.comp = comp;
+    }
+    SB_TRY(launch_stage(a, P, o->n_state, o->order, kind, stage == 1, h->stream));
+    if (stage == 1 && o->scheme == 1) h->cur = 1 - h->cur;
+    return SETB_OK;
+}
+
+int32_t setb_slab_view(setb_handle* h, int32_t stage, double** base, int64_t* var_stride, int64_t* plane_stride,
+                       int32_t* nz_buffer) {
+    if (!h || !h->g.kb || (stage != 1 && stage != 2) || !base || !var_stride || !plane_stride || !nz_buffer)
+        return SETB_EINVAL;
+    *base = h->buf[stage == 1 ? h->cur : 1 - h->cur];
+    *var_stride = h->g.vs;
+    *plane_stride = h->g.ps;
+    *nz_buffer = h->g.nz;
+    return SETB_OK;
+}
+
+int32_t setb_slab_dt(setb_handle* h, double** dt_next) {
+    if (!h || !h->g.kb || !dt_next) return SETB_EINVAL;
+    *dt_next = &h->clk->dt_cur;
     return SETB_OK;
 }
 

@@ -51,6 +51,10 @@ struct DevStatus {
 // Geometry + boundary data of one Cartesian grid.
 struct GridGeom {
     int nx, ny, nz, lz;             // lz: z extent of one CTA's march
+    int kb, ke, koff;               // z slab: the stage kernels update planes [kb, ke) of the nz
+                                    // held (ke = 0: all nz), the others are ghost planes filled by
+                                    // the caller; buffer plane k is plane k + koff of the whole
+                                    // grid (source-sphere geometry, first-bad-cell index)
     long long vs, ps, px;           // var / plane / row strides of the SoA state (elements);
                                     // device-owned states keep px even and vs a multiple of 32
                                     // (16-byte rows for the tensor copies, 256-byte planes)
@@ -61,6 +65,12 @@ struct GridGeom {
     double inflow[8];               // primitive ghost state beyond x = hi
     double r_src, rho_src, v_src, p_over_rho_src, r_floor;
 };
+
+// Ghost planes on each side of a z slab (the reconstruction stencil reaches two planes).
+constexpr int kSlabGhost = 2;
+// Updated plane range [kb, ke) of a geometry.
+SB_HD int plane_begin(const GridGeom& g) { return g.kb; }
+SB_HD int plane_end(const GridGeom& g) { return g.ke > 0 ? g.ke : g.nz; }
 
 struct StageArgs {
     GridGeom g;

@@ -259,8 +259,9 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     const int t = threadIdx.x;
     const int tx = t % TX, ty = t / TX;
     const int i0 = bx * TX, j0 = by * TY;
-    const int k0 = bz * g.lz;
-    const int k1 = min(g.nz, k0 + g.lz);
+    const int kb = plane_begin(g), ke = plane_end(g);
+    const int k0 = kb + bz * g.lz;
+    const int k1 = min(ke, k0 + g.lz);
     const double dt = A.clk->dt_cur;
     if (t < 5) cnt[t] = 0;
 
@@ -303,7 +304,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             oidx = c;
             ostride = PLANE;
             gk = k + 1;
-            real = (i0 + fxx < g.nx) && (j0 + fyy < g.ny) && (k + 1 <= g.nz) && (k + 1 >= 0);
+            real = (i0 + fxx < g.nx) && (j0 + fyy < g.ny) && (k + 1 <= ke) && (k + 1 >= kb);
         } else if (job < JX) {
             axis = 0;
             if (job < 2 * TY) {
@@ -419,7 +420,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         if (k < k0 - 1) continue;
         const bool pro = (k < k0);
         const int njobs = pro ? JZ : JOBS;
-        for (int job = warp; job < njobs; job += NW) do_face(job, k, pro && k0 > 0);
+        for (int job = warp; job < njobs; job += NW) do_face(job, k, pro && k0 > kb);
         double fzh[8];
         {
             const RG* zk = ring + ring_slot(k - 1) * 8 * PLANE + (ty + 2) * HX + tx + 2;
@@ -438,7 +439,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             bool reset_comp = false;
             bool is_src = false;
             if (col_src) {   // (x^2 + y^2) + z^2 < r_src^2, rounded as in source_prim
-                const double cz = cell_coord(g.lo[2], k, g.h[2]);
+                const double cz = cell_coord(g.lo[2], k + g.koff, g.h[2]);
                 const double r2 = dadd(xy2, dmul(cz, cz));
                 if (r2 < rsrc2) {
                     source_state(g, cxs, cys, cz, r2, qs);
@@ -478,7 +479,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                 }
                 if (!(un[0] > 0.0)) {                    // cuf_solvers.cuf:708-711
                     atomicAdd(&cnt[0], 1ull);
-                    atomicMin(&A.st->first_bad, (unsigned long long)(gi + (long long)g.nx * (gj + (long long)g.ny * k)));
+                    atomicMin(&A.st->first_bad,
+                              (unsigned long long)(gi + (long long)g.nx * (gj + (long long)g.ny * (k + g.koff))));
 #pragma unroll
                     for (int v = 0; v < 8; v++) un[v] = uin[v];
                     reset_comp = true;
@@ -611,7 +613,8 @@ cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
         attr_set = true;
     }
     constexpr int TX = Tile<P, KIND>::TX, TY = Tile<P, KIND>::TY;
-    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, (a.g.nz + a.g.lz - 1) / a.g.lz);
+    const int nzu = plane_end(a.g) - plane_begin(a.g);
+    dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY, (nzu + a.g.lz - 1) / a.g.lz);
     kern<<<grid, Tile<P, KIND>::NT, smem, s>>>(a);
     return cudaGetLastError();
 }

@@ -89,3 +89,19 @@ def test_solver_needs_a_gpu():
     with pytest.raises(S.SetbError) as e:
         S.Solver(S.cart_desc(8))
     assert e.value.code == 8   # SETB_ENODEV: no CPU fallback
+
+
+def test_slab_arguments_checked_on_the_host():
+    """setb_init_slab validates the slab against the grid before touching a device."""
+    from set_b200 import slab as SL
+    desc = S.cart_desc((8, 6, 10))
+    cp = np.zeros((8 * 6 * 4, 16))
+    L = S.lib()
+    h = C.c_void_p()
+    for k0, n in ((0, 1), (-1, 4), (8, 4), (7, 4)):
+        assert L.setb_init_slab(C.byref(h), C.byref(desc), k0, n, cp.ctypes.data_as(C.POINTER(C.c_double))) == 1
+    if not has_gpu():
+        assert L.setb_init_slab(C.byref(h), C.byref(desc), 2, 4, cp.ctypes.data_as(C.POINTER(C.c_double))) == 8
+    assert SL.split_z(10, 3) == [(0, 4), (4, 3), (7, 3)]
+    with pytest.raises(ValueError):
+        SL.split_z(5, 3)
