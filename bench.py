@@ -229,6 +229,7 @@ def run_slab(args, world, rank, local):
     if world > 1:
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        torch.distributed.barrier()   # a group-wide collective before the first point-to-point batch
     n, T = args.n, args.tsteps
     nz = n * world
     desc = S.cart_desc((n, n, nz))
