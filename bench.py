@@ -272,7 +272,7 @@ def run_slab(args, world, rank, local):
     diag = slab.status()
     cells = n * n * nz
     if rank == 0:
-        line = {"metric": "mhd_cell_updates_per_s", "value": cells * T * args.steps / (ms / 1e3),
+        line = {"metric": "cell_updates_per_s", "value": cells * T * args.steps / (ms / 1e3),
                 "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic (LISM + solar-wind source, seeded)",
