@@ -475,7 +475,10 @@ def run_ours(args, world, rank, local):
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum at 160^3, "
                                            "scaled by cells",
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
-                         "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2}},
+                         "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
+                         "limiter": "FP64 latency and issue, not DRAM: at 160^3 ncu shows DRAM traffic 0.98x "
+                                    "algorithmic, FP64 pipe 40-42 %, issue 50-53 % at 12 warps/SM "
+                                    "(profiles/stage_plain_hlld_160cube.md)"},
             "mixed": mixed,
             "ensemble": ensemble,
             "served": served,
