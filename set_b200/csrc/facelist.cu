@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
                                    dmul(n[2], dadd(q1[7], q2[7])));
             m.divb[gr] = dmul(dmul(0.5, nb), sq);
         }
-        if (WANT_DT) cand = fmin(kDtFaceCap, cfl * dist / fmax(fabs(sp[0]), fabs(sp[1])));
+        if (WANT_DT) cand = fmin(kDtFaceCap, cfl * dist * sb_rcp(fmax(fabs(sp[0]), fabs(sp[1]))));
     }
     if (n_recon) atomicAdd(&cnt[0], (unsigned long long)n_recon);
     if (n_wave) atomicAdd(&cnt[1], (unsigned long long)n_wave);
@@ -400,13 +400,15 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
                     pot[4] = dadd(pot[4], dmul(ub / kCpi4, sks));
                 }
             }
-            const double vol = m.cell_volume[c];
+            // one reciprocal of the volume instead of eight divisions (the face-list path measured
+            // 7 % faster); the dt candidate below likewise multiplies by 1/max(|SL|,|SR|)
+            const double ivol = sb_rcp(m.cell_volume[c]);
             double uin[8];
 #pragma unroll
             for (int v = 0; v < 8; v++) {
                 uin[v] = Uin[v * vs + c];
-                if (KIND == 0) un[v] = uin[v] - dt * (pot[v] / vol);
-                else un[v] = 0.5 * ((Ubase[v * vs + c] + uin[v]) - dt * (pot[v] / vol));
+                if (KIND == 0) un[v] = uin[v] - dt * (pot[v] * ivol);
+                else un[v] = 0.5 * ((Ubase[v * vs + c] + uin[v]) - dt * (pot[v] * ivol));
             }
             if (!(un[0] > 0.0)) {
                 atomicAdd(&cnt[0], 1ull);
