@@ -322,7 +322,10 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
 // of the face fluxes (:691-703), Euler / Heun stage (:705-770), negative-density check, p floor
 // (:777-779), frozen cells (:611) and the re-imposed source sphere.  The last block of a
 // finalizing launch rolls the clock.
-template <int KIND>
+// PHYS: the physics option; POWELL: the div-B terms are on (their energy term by m.powell ==
+// 2).  Compile-time, so a launch carries only its own code (registers set the occupancy of this
+// gather-bound kernel).
+template <int KIND, int PHYS, bool POWELL>
 __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev m, const double* __restrict__ Uin,
                                                                const double* Ubase, double* Uout, int64_t vs,
                                                                DevClock* clk, DevStatus* st, int finalize) {
@@ -339,10 +342,10 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
         if (m.cell_flag[c] & 1) {
 #pragma unroll
             for (int v = 0; v < 8; v++) un[v] = KIND == 0 ? Uin[v * vs + c] : Ubase[v * vs + c];
-        } else if (m.physics == 0 && m.src.r_src > 0.0 && r2 < dmul(m.src.r_src, m.src.r_src)) {
+        } else if (PHYS == 0 && m.src.r_src > 0.0 && r2 < dmul(m.src.r_src, m.src.r_src)) {
             source_state(m.src, x, y, z, r2, qs);
             cons_from_prim_exact(qs, un);
-        } else if (m.physics == 1) {
+        } else if (PHYS == 1) {
             double pot[8];
 #pragma unroll
             for (int v = 0; v < 8; v++) pot[v] = 0.0;
@@ -382,9 +385,9 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
                     pot[2 * v] = owner ? pot[2 * v] + d.x : pot[2 * v] - d.x;
                     pot[2 * v + 1] = owner ? pot[2 * v + 1] + d.y : pot[2 * v + 1] - d.y;
                 }
-                if (m.powell) sks = owner ? sks + m.divb[jf] : sks - m.divb[jf];
+                if (POWELL) sks = owner ? sks + m.divb[jf] : sks - m.divb[jf];
             }
-            if (m.powell) {
+            if (POWELL) {
                 // div-B sources inside the flux sum (cuf_solvers.cuf:529-533 / 729-733, commented
                 // there): momentum + (B/4pi) sks, B + u sks, powell 2 energy + (u.B/4pi) sks, with
                 // u and B of the stage input (the primitive pass of this stage)
@@ -670,8 +673,18 @@ cudaError_t fl_launch_stage(const FaceListDev* f, const double* Uin, const doubl
         default: launch_face_n<3>(m, o->order, want_dt, o->cfl, o->n_disc, clk, st, s); break;
     }
     const unsigned cgrid = (unsigned)((m.n_cell + kCellThreads - 1) / kCellThreads);
-    if (kind == 0) fl_cell_kernel<0><<<cgrid, kCellThreads, 0, s>>>(m, Uin, Ubase, Uout, vs, clk, st, finalize);
-    else fl_cell_kernel<1><<<cgrid, kCellThreads, 0, s>>>(m, Uin, Ubase, Uout, vs, clk, st, finalize);
+#define SB_CELL(K, PH, PW) fl_cell_kernel<K, PH, PW><<<cgrid, kCellThreads, 0, s>>>(m, Uin, Ubase, Uout, vs, clk, st, finalize)
+    if (m.physics == 1) {
+        if (kind == 0) SB_CELL(0, 1, false);
+        else SB_CELL(1, 1, false);
+    } else if (m.powell) {
+        if (kind == 0) SB_CELL(0, 0, true);
+        else SB_CELL(1, 0, true);
+    } else {
+        if (kind == 0) SB_CELL(0, 0, false);
+        else SB_CELL(1, 0, false);
+    }
+#undef SB_CELL
     return cudaGetLastError();
 }
 
