@@ -449,7 +449,7 @@ def run_ours(args, world, rank, local):
                   "sequential_plain_solves_per_s": seq["solves_per_s"],
                   "speedup_vs_sequential_plain": out["solves_per_s"] / seq["solves_per_s"]}
 
-    # ---- the face-list path (SURVEY "next" row: the reference's geometry) on a 128^3 box
+    # ---- the face-list path (the reference's own grid geometry) on a 128^3 box
     facelist = None
     if rank == 0 and world == 1 and args.facelist_n > 0:
         facelist = [facelist_leg(args.facelist_n, 50, False), facelist_leg(args.facelist_n, 50, True)]
