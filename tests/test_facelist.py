@@ -232,3 +232,19 @@ def test_powell_option_is_validated_on_the_host():
         with pytest.raises(S.SetbError) as e:
             FL.FaceListSolver(m, cp, params)
         assert e.value.code == 1
+
+
+@pytest.mark.parametrize("powell", [1, 2])
+def test_oracle_powell_keeps_mass_conservation(powell):
+    """The div-B sources act on momentum, B (and energy) only: in a closed box mass is conserved
+    to round-off over Heun steps with a non-solenoidal field."""
+    walls = {k: 2 for k in ("x-", "x+", "y-", "y+", "z-", "z+")}
+    m = FL.box_facelist((6, 5, 4), stretch=0.4, sides=walls, seed=3, permute_seed=2)
+    cp = _nonsolenoidal_cellpar(m, 4)
+    U0 = O.cellpar_to_cons(cp, (m.n_cell,)).reshape(8, -1)
+    U = U0.copy()
+    _, dg, _ = O.fl_run(O.facelist(m, FL.fl_params(r_src=0.0, dt_init=1e-3, powell=powell)),
+                        O.make_opts(3, 2, 2, 0.4), U, 8)
+    tot0, tot = (U0[0] * m.cell_volume).sum(), (U[0] * m.cell_volume).sum()
+    assert abs(tot - tot0) <= 1e-13 * abs(tot0)
+    assert dg.n_negdens == 0
