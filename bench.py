@@ -113,9 +113,9 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_baseline(n: int, tsteps_sample: int = 1):
-    """The oracle (CPU port of the reference algorithm) on all host threads: one RK2 HLLD step
-    of the n^3 grid; returns cell-updates/s and the thread count."""
+def cpu_baseline(n: int, tsteps_sample: int = 1, threads: int = 0):
+    """The oracle (CPU port of the reference algorithm) on `threads` host threads (0 = all): one
+    RK2 HLLD step of the n^3 grid; returns cell-updates/s, the thread count and the seconds."""
     import numpy as np  # noqa: F401
     import oracle as O
     O.build()
@@ -123,7 +123,7 @@ def cpu_baseline(n: int, tsteps_sample: int = 1):
     U = O.init_lism(g, seed=2)
     ck = O.clock_init(g)
     ck.dt_next = 1e-4
-    threads = O.max_threads()
+    threads = threads or O.max_threads()
     t0 = time.perf_counter()
     O.run(g, O.make_opts(3, 2, 2, 0.4), U, tsteps_sample, ck, nthreads=threads)
     dt = time.perf_counter() - t0
@@ -457,8 +457,11 @@ def run_ours(args, world, rank, local):
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, thr, secs = cpu_baseline(n)
+        v1, _, secs1 = cpu_baseline(64, threads=1)
         base = {"value": v, "unit": "cell-updates/s", "cores": thr, "kind": "port",
-                "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid ({secs:.1f} s)"}
+                "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid ({secs:.1f} s)",
+                "single_thread": {"value": v1, "unit": "cell-updates/s", "cores": 1,
+                                  "sample": f"1 RK2 HLLD minmod step of the 64^3 grid ({secs1:.1f} s)"}}
 
     if rank == 0:
         line = {
