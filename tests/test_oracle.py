@@ -180,3 +180,28 @@ def test_lagged_dt_semantics():
     assert 1e-6 < dt2 < 1.0
     ck, _ = O.run(g, O.make_opts(), U, 1, ck)
     assert ck.dt_last == dt2 and ck.time_all == 2e-9 + dt2
+
+
+@pytest.mark.parametrize("n_state", [1, 2, 3])
+def test_wave_speeds_are_galilean_invariant(n_state):
+    """Shifting both states' normal velocity by V shifts SL, SR and SM by V (n_disc = 0: the
+    Davis estimates and SM depend on S - v only), for the oracle and the product's host chlld."""
+    import set_b200 as S
+    rng = np.random.default_rng(400 + n_state)
+    for t in range(200):
+        q1, q2 = rand_state(rng, 0.0 if n_state == 2 else 2.0), rand_state(rng, 0.0 if n_state == 2 else 2.0)
+        n = rng.normal(size=3)
+        n /= np.linalg.norm(n)
+        V = float(rng.normal(0, 3.0))
+        s1, s2 = q1.copy(), q2.copy()
+        s1[1:4] += V * n
+        s2[1:4] += V * n
+        rc, _, sl, sp, sc = O.chlld(n_state, n, 0.0, q1, q2)
+        rcs, _, sls, sps, scs = O.chlld(n_state, n, 0.0, s1, s2)
+        assert rc == 0 and rcs == 0
+        scale = max(abs(sl), abs(sp), abs(V), 1.0)
+        for a, b in ((sls, sl), (sps, sp), (scs, sc)):
+            assert abs(a - (b + V)) <= 1e-12 * scale
+        _, hsl, hsp, hsc = S.chlld(n_state, n, 0.0, s1, s2)
+        for a, b in ((hsl, sl), (hsp, sp), (hsc, sc)):
+            assert abs(a - (b + V)) <= 1e-12 * scale
