@@ -420,6 +420,7 @@ int32_t setb_batch_remove(setb_batch* b, int32_t slot) {
 }
 
 int32_t setb_batch_step(setb_batch* b, int32_t nsteps) {
+    NvtxRange range("setb_batch_step");
     if (!b || nsteps < 0) return SETB_EINVAL;
     cudaSetDevice(b->device);
     int rc = run_steps(b, nsteps);

@@ -13,11 +13,16 @@
 #include <new>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "setb200.h"
 #include "setb_internal.cuh"
 #include "chlld_q.cuh"
 
 using namespace sb;
+
+sb::NvtxRange::NvtxRange(const char* name) { nvtxRangePushA(name); }
+sb::NvtxRange::~NvtxRange() { nvtxRangePop(); }
 
 struct setb_handle {
     int device = 0;
@@ -465,6 +470,7 @@ int32_t setb_cart_fill_lism(const setb_cart_desc* d, const setb_lism_ic* ic, dou
 }
 
 int32_t setb_init_cartesian(setb_handle** out, const setb_cart_desc* d, const double* cell_par) {
+    NvtxRange range("setb_init_cartesian");
     if (!cell_par) return SETB_EINVAL;
     int rc = create_impl(out, d);
     if (rc) return rc;
@@ -655,6 +661,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
 }  // namespace
 
 int32_t setb_step(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all) {
+    NvtxRange range("setb_step");
     if (!h || nsteps < 0 || h->g.kb) return SETB_EINVAL;   // a z slab steps stage by stage
     int rc = validate_opts(o);
     if (rc) return rc;
@@ -672,6 +679,7 @@ int32_t setb_step(setb_handle* h, int32_t nsteps, const setb_step_opts* o, doubl
 
 int32_t setb_step_profiled(setb_handle* h, int32_t nsteps, const setb_step_opts* o, double* time_all,
                            double kernel_ms[2], int32_t launches[2]) {
+    NvtxRange range("setb_step_profiled");
     if (!h || nsteps < 0 || !kernel_ms || !launches || h->g.kb) return SETB_EINVAL;
     int rc = validate_opts(o);
     if (rc) return rc;
@@ -715,6 +723,7 @@ int32_t setb_sync(setb_handle* h) {
 }
 
 int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_all) {
+    NvtxRange range("setb_get_state");
     if (!h || !cell_par) return SETB_EINVAL;
     cudaSetDevice(h->device);
     const size_t N = (size_t)h->g.nx * h->g.ny * h->g.nz;
@@ -738,6 +747,7 @@ int32_t setb_get_state(setb_handle* h, double* cell_par, double* time_all) {
 }
 
 int32_t setb_set_state(setb_handle* h, const double* cell_par, double time_all) {
+    NvtxRange range("setb_set_state");
     if (!h || !cell_par) return SETB_EINVAL;
     cudaSetDevice(h->device);
     SB_TRY(cudaStreamSynchronize(h->stream));
@@ -847,6 +857,7 @@ int32_t setb_init_slab(setb_handle** h, const setb_cart_desc* d, int32_t k0, int
 }
 
 int32_t setb_slab_stage(setb_handle* h, int32_t stage, const setb_step_opts* o) {
+    NvtxRange range("setb_slab_stage");
     if (!h || !h->g.kb || (stage != 1 && stage != 2)) return SETB_EINVAL;
     int rc = validate_opts(o);
     if (rc) return rc;

@@ -66,6 +66,15 @@ struct GridGeom {
     double r_src, rho_src, v_src, p_over_rho_src, r_floor;
 };
 
+// Scoped NVTX range on the host (header-only NVTX3: a no-op unless a profiler or tracer attaches),
+// named after the C entry point, so timelines and ncu --nvtx filters show the library's calls.
+struct NvtxRange {
+    explicit NvtxRange(const char* name);
+    ~NvtxRange();
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 // Ghost planes on each side of a z slab (the reconstruction stencil reaches two planes).
 constexpr int kSlabGhost = 2;
 // Updated plane range [kb, ke) of a geometry.
