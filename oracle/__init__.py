@@ -3,15 +3,19 @@
 ctypes front end of the CPU FP64 oracle (oracle/oracle.cpp), a restatement of SergeyMSU/SET's
 MHD step (SET_Fortran_Cuda_MHD/Solvers.f90:1144-1859 chlld, :109-150 minmod/linear;
 cuf_solvers.cuf:243-794 face/cell kernels; cuf_kernel.cuf:780-925 time loop) on a Cartesian
-grid, plus the reference's own C++ HLL solver (SET_Gelios/source/Solvers.cpp:92-691) built
-into oracle/_ref for pinning.
+grid, plus the reference's own C++ Riemann solvers (SET_Gelios/source/Solvers.cpp: the HLL
+HLLD_Solver_Alexashov :92-691, the HLLC HLLC_Aleksashov :1324-1639 and the HLLD HLLDQ_Korolkov
+:1642-2185) built into oracle/_ref for pinning and cross-checks.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.  The
 product (set_b200) never does.
 
-Parity status: the HLL branch of chlld is pinned against the compiled reference C++ solver;
-the HLLC/HLLD branches and the Cartesian driver are parity unpinned (the reference has no
-tests or golden vectors, and its Fortran path cannot be compiled without a Fortran compiler).
+Parity status: chlld's shared set-up and HLL branch are pinned bit for bit against the compiled
+reference C++ HLL solver, and its HLLC branch (B = 0) bit for bit against the reference's C++
+HLLC; its HLLD branch is cross-checked to 1e-10 against the reference's second HLLD
+(HLLDQ_Korolkov, axis-aligned faces).  The Cartesian and face-list drivers are restatements of
+cuf_solvers.cuf checked by properties (the reference has no tests, and its Fortran path cannot be
+compiled without a Fortran compiler).
 """
 from __future__ import annotations
 
@@ -99,6 +103,10 @@ def ref_lib():
         _ref = C.CDLL(_REF)
         _ref.ref_gelios_hll.restype = C.c_double
         _ref.ref_gelios_hll.argtypes = [_dp, _dp, _dp, C.c_double, C.c_double, _dp, _dp, _dp, _dp]
+        _ref.ref_gelios_hllc.restype = C.c_double
+        _ref.ref_gelios_hllc.argtypes = [_dp, _dp, _dp, C.c_double, _dp]
+        _ref.ref_korolkov.restype = C.c_double
+        _ref.ref_korolkov.argtypes = [C.c_int, _dp, C.c_double, _dp, C.c_double, _dp, C.c_double, _dp, _dp]
     return _ref
 
 
@@ -144,6 +152,30 @@ def ref_hll(normal, w, q1, q2, dist=1.0):
     ref_lib().ref_gelios_hll(_p(q1), _p(q2), _p(n), float(w), float(dist), _p(out), C.byref(dsl),
                              C.byref(dsp), C.byref(dsc))
     return out, dsl.value, dsp.value, dsc.value
+
+
+def ref_hllc(normal, q1, q2):
+    """The reference's own C++ HLLC solver (Solvers.cpp:1324-1639; B = 0, fixed face): returns the
+    five fluxes (rho, mx, my, mz, E).  The B entries of q1/q2 are ignored."""
+    q1 = np.ascontiguousarray(q1, dtype=np.float64)
+    q2 = np.ascontiguousarray(q2, dtype=np.float64)
+    n = np.ascontiguousarray(normal, dtype=np.float64)
+    out = np.zeros(5)
+    ref_lib().ref_gelios_hllc(_p(q1), _p(q2), _p(n), 1.0, _p(out))
+    return out
+
+
+def ref_korolkov(metod, normal, q1, q2, Q1=0.0, Q2=0.0):
+    """The reference's HLLDQ_Korolkov (Solvers.cpp:1642-2185; metod 3 = HLLD, 2 = its HLLC
+    variant) on an axis-aligned normal, w = 0: returns (qqq[8] in chlld's order, passive-scalar
+    flux)."""
+    q1 = np.ascontiguousarray(q1, dtype=np.float64)
+    q2 = np.ascontiguousarray(q2, dtype=np.float64)
+    n = np.ascontiguousarray(normal, dtype=np.float64)
+    out = np.zeros(8)
+    pq = C.c_double()
+    ref_lib().ref_korolkov(int(metod), _p(q1), float(Q1), _p(q2), float(Q2), _p(n), 1.0, _p(out), C.byref(pq))
+    return out, pq.value
 
 
 def minmod(x, y):

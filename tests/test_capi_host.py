@@ -62,6 +62,27 @@ def test_host_chlld_reference_golden_hll():
         assert np.abs(f - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
+def test_host_chlld_reference_golden_hllc():
+    """HLLC on B = 0 faces against the reference's own C++ HLLC (Solvers.cpp:1324-1639)."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "gelios_hllc.npz"))
+    for k in range(g["q1"].shape[0]):
+        f, *_ = S.chlld(2, g["normal"][k], 0.0, g["q1"][k], g["q2"][k])
+        ref = g["qqq5"][k]
+        assert np.abs(f[:5] - ref).max() <= 1e-12 * np.abs(ref).max()
+        assert np.abs(f[5:]).max() == 0.0
+
+
+def test_host_chlld_cross_check_korolkov_hlld():
+    """HLLD against the reference's HLLDQ_Korolkov (metod 3) outside chlld's last-match-wins
+    region: |dF| <= 1e-10 max|F| per face (the two solvers' operation orders differ)."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "korolkov_hlld.npz"))
+    errs = []
+    for k in np.nonzero(g["quirk"] == 0)[0]:
+        f, *_ = S.chlld(3, g["normal"][k], 0.0, g["q1"][k], g["q2"][k])
+        errs.append(np.abs(f - g["qqq"][k]).max() / np.abs(g["qqq"][k]).max())
+    assert max(errs) <= 1e-10 and np.median(errs) <= 1e-14
+
+
 def test_host_chlld_rejects_bad_arguments():
     q = np.array([1.0, 0, 0, 0, 1.0, 0, 0, 0])
     with pytest.raises(S.SetbError) as e:

@@ -86,6 +86,27 @@ def test_chlld_batch_reference_golden_hll():
     assert err.max() <= 1e-12
 
 
+def test_chlld_batch_reference_golden_hllc():
+    """The GPU HLLC on B = 0 faces against the reference's own C++ HLLC (Solvers.cpp:1324-1639)."""
+    g = np.load(__file__.replace("test_gpu_parity.py", "golden/gelios_hllc.npz"))
+    qqq, sp, fl = S.chlld_batch(2, g["normal"], g["q1"], g["q2"], w=np.zeros(len(g["q1"])))
+    assert (fl & 1).sum() == 0
+    err = np.abs(qqq[:, :5] - g["qqq5"]).max(axis=1) / np.abs(g["qqq5"]).max(axis=1)
+    assert err.max() <= 1e-12
+    assert np.abs(qqq[:, 5:]).max() == 0.0
+
+
+def test_chlld_batch_cross_check_korolkov_hlld():
+    """The GPU HLLD against the reference's HLLDQ_Korolkov (metod 3) outside chlld's
+    last-match-wins region: |dF| <= 1e-10 max|F| per face, median <= 1e-14."""
+    g = np.load(__file__.replace("test_gpu_parity.py", "golden/korolkov_hlld.npz"))
+    keep = g["quirk"] == 0
+    qqq, sp, fl = S.chlld_batch(3, g["normal"][keep], g["q1"][keep], g["q2"][keep], w=np.zeros(keep.sum()))
+    ref = g["qqq"][keep]
+    err = np.abs(qqq - ref).max(axis=1) / np.abs(ref).max(axis=1)
+    assert err.max() <= 1e-10 and np.median(err) <= 1e-14
+
+
 @pytest.mark.parametrize("n_state", [0, 1, 2, 3])
 @pytest.mark.parametrize("ydar", [False, True])
 def test_chlld_q_batch_matches_oracle(n_state, ydar):

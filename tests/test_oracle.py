@@ -1,8 +1,12 @@
-"""The CPU oracle: pinned against the reference's own compiled solver, plus property tests.
+"""The CPU oracle: pinned against the reference's own compiled solvers, plus property tests.
 
-The reference ships no tests.  Its C++ HLL solver (SET_Gelios/source/Solvers.cpp:92-691) pins
-chlld's shared set-up and HLL branch; HLLC/HLLD and the Cartesian driver are checked by
-properties the reference's algorithm must have.
+The reference ships no tests.  Three of its C++ Riemann solvers (SET_Gelios/source/Solvers.cpp)
+compile here and pin the oracle's chlld:
+  * HLLD_Solver_Alexashov (:92-691, HLL) -- the shared set-up and the HLL branch, bit for bit;
+  * HLLC_Aleksashov (:1324-1639) -- the HLLC branch on B = 0 states, bit for bit;
+  * HLLDQ_Korolkov (:1642-2185, metod 3) -- a second author's HLLD, a tolerance cross-check of
+    the HLLD branch on the axis-aligned faces where both use the same wave-speed estimate.
+The Cartesian driver is checked by properties the reference's algorithm must have.
 """
 import os
 
@@ -12,6 +16,11 @@ import pytest
 import oracle as O
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden", "gelios_hll.npz")
+GOLD_HLLC = os.path.join(os.path.dirname(__file__), "golden", "gelios_hllc.npz")
+GOLD_HLLD = os.path.join(os.path.dirname(__file__), "golden", "korolkov_hlld.npz")
+# chlld (HLLD) against HLLDQ_Korolkov outside the quirk region: the two differ in operation order
+# (fast speeds, star states, energies), so |dF| <= 1e-10 max|F| per face and a median of 1e-14.
+KOROLKOV_TOL = 1e-10
 
 
 def phys_flux(q, n):
@@ -61,6 +70,96 @@ def test_hll_matches_reference_live():
         g, rsl, rsp, rsc = O.ref_hll(n, 0.0, q1, q2)
         np.testing.assert_array_equal(f, g)
         n_done += 1
+
+
+def test_hllc_matches_reference_golden_vectors():
+    """chlld n_state 2 on B = 0 faces (Solvers.f90:1465-1596) equals the reference's C++ HLLC
+    bit for bit: the same basis fallback, Davis speeds, SM, ptz average and star states."""
+    g = np.load(GOLD_HLLC)
+    assert g["q1"].shape[0] >= 800 and set(np.unique(g["kind"])) == {0, 1, 2, 3}
+    for k in range(g["q1"].shape[0]):
+        rc, f, sl, sp, sc = O.chlld(2, g["normal"][k], 0.0, g["q1"][k], g["q2"][k])
+        assert rc == 0
+        np.testing.assert_array_equal(f[:5], g["qqq5"][k])
+        assert not f[5:].any()   # no field: the B fluxes are zero
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference tree absent)")
+def test_hllc_matches_reference_live():
+    rng = np.random.default_rng(17)
+    for t in range(400):
+        q1, q2 = rand_state(rng, 0.0), rand_state(rng, 0.0)
+        n = np.eye(3)[rng.integers(3)] * rng.choice([-1.0, 1.0]) if t % 2 else rng.normal(size=3)
+        n = n / np.linalg.norm(n)
+        rc, f, *_ = O.chlld(2, n, 0.0, q1, q2)
+        assert rc == 0
+        np.testing.assert_array_equal(f[:5], O.ref_hllc(n, q1, q2))
+
+
+def korolkov_errors(fn):
+    """Per-face |dF| / max|F| of fn(normal, q1, q2) -> 8 fluxes against the Korolkov vectors,
+    and the quirk mask."""
+    g = np.load(GOLD_HLLD)
+    err = np.array([np.abs(fn(g["normal"][k], g["q1"][k], g["q2"][k]) - g["qqq"][k]).max() / np.abs(g["qqq"][k]).max()
+                    for k in range(g["q1"].shape[0])])
+    return err, g["quirk"] == 1
+
+
+def test_hlld_cross_check_korolkov_golden():
+    """chlld n_state 3 against the reference's second HLLD (HLLDQ_Korolkov metod 3) on faces
+    where both estimate SL/SR alike.  Outside chlld's last-match-wins region they agree to
+    rounding; inside it they select different fan regions by construction."""
+    err, quirk = korolkov_errors(lambda n, a, b: O.chlld(3, n, 0.0, a, b)[1])
+    assert (~quirk).sum() >= 800 and quirk.sum() >= 20
+    assert err[~quirk].max() <= KOROLKOV_TOL, err[~quirk].max()
+    assert np.median(err[~quirk]) <= 1e-14
+    assert err[quirk].min() > 1e-3
+
+
+def test_hlld_korolkov_quirk_faces():
+    """The quirk region, face by face.  With SL > 0 > SZL, HLLDQ_Korolkov's forward else-if chain
+    stops at its first block (the left state's physical flux) while chlld's sequential IF blocks
+    end in the L** block.  With SR < 0 < SZR it is the other way round: HLLDQ_Korolkov takes its
+    R** block (SM < 0 < SRR) before reaching SR <= 0, while chlld's last block, SR < 0, leaves the
+    right state's physical flux.  The upwind physical flux, with the normal-B flux of both solvers
+    (-SN (bnR - bnL)), is therefore Korolkov's answer on the left and chlld's on the right."""
+    g = np.load(GOLD_HLLD)
+    sides = set()
+    for k in np.nonzero(g["quirk"])[0]:
+        n, q1, q2 = g["normal"][k], g["q1"][k], g["q2"][k]
+        rc, f, sl, sp, sm = O.chlld(3, n, 0.0, q1, q2)
+        F = phys_flux(q1 if sl > 0 else q2, n)
+        F[5:8] += (g["qqq"][k][5:8] @ n - F[5:8] @ n) * n
+        upwind = g["qqq"][k] if sl > 0 else f
+        np.testing.assert_allclose(upwind, F, rtol=1e-11, atol=1e-11 * np.abs(F).max())
+        sides.add(sl > 0)
+    assert sides == {True, False}
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference tree absent)")
+def test_hlld_cross_check_korolkov_live():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import hlld_fan
+    rng = np.random.default_rng(29)
+    done = 0
+    errs = []
+    while done < 400:
+        n = np.eye(3)[rng.integers(3)] * rng.choice([-1.0, 1.0])
+        ax = int(np.argmax(np.abs(n)))
+        q1, q2 = rand_state(rng), rand_state(rng)
+        if done % 2:
+            q2[[0, 4]], q2[5:8] = q1[[0, 4]], q1[5:8] * np.where(np.arange(3) == ax, 1.0, -1.0)
+        else:
+            q2[1 + ax] = q1[1 + ax]
+        rc, f, sl, sp, sc = O.chlld(3, n, 0.0, q1, q2)
+        bn, ttL, ttR, szl, szr = hlld_fan(n, q1, q2, sl, sp, sc)
+        if (sl > 0 > szl) or (sp < 0 < szr) or 1e-6 < abs(bn) <= 1e-3 or min(abs(ttL), abs(ttR)) < 1e-6:
+            continue
+        g, _ = O.ref_korolkov(3, n, q1, q2)
+        errs.append(np.abs(f - g).max() / np.abs(g).max())
+        done += 1
+    assert max(errs) <= KOROLKOV_TOL and np.median(errs) <= 1e-14
 
 
 def test_minmod_linear_known_answers():
