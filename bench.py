@@ -15,8 +15,12 @@ Prints one JSON line on rank 0.
   roofline  per-kernel CUDA-event times over the timed region (setb_step_profiled); algorithmic
             bytes per cell-update: 128 B for the first stage (read U^n, write U*), 192 B for the
             second (read U*, U^n, write U^n+1).
-  cpu_baseline  the CPU oracle (a port of the reference algorithm) on this host's cores, one
-            RK2 step of the same grid.
+  c3        config C3: one seeded Mach/beta draw at 384^3 x 500 steps, the mixed form against
+            plain FP64 (speed-up, L1 of rho, p, |B|, total-energy drift).
+  cpu_baseline  the CPU oracle (a port of the reference algorithm) on this host's cores: one
+            RK2 step of the same grid, plus the 96^3 parity grid and config C1 (64^3, first
+            order, forward Euler) at all threads and one thread.
+`--c5 K` runs config C5 at its stated parameters on K requests instead (one JSON line).
 N > 1 runs N independent replicas (weak scaling): no data-path collective.
 """
 from __future__ import annotations
@@ -37,9 +41,9 @@ sys.path.insert(0, ROOT)
 BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
 BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
 BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
-# DRAM bytes (read + write) per cell of one plain stage-2 launch, from the ncu capture at 160^3
-# summarised in profiles/stage_plain_hlld_160cube.md (774.07 MB / 4.096 M cells); traffic grows
-# with the cell count, so the full-size launch's traffic is this figure times its cells.
+# DRAM bytes (read + write) per cell of one plain stage-2 launch, from an ncu capture of that
+# kernel at 160^3 (774.07 MB / 4.096 M cells); traffic grows with the cell count, so the
+# full-size launch's traffic is this figure times its cells.
 TRAFFIC_STAGE2_PER_CELL = 774.065152e6 / 160 ** 3
 
 
@@ -113,21 +117,43 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_baseline(n: int, tsteps_sample: int = 1, threads: int = 0):
-    """The oracle (CPU port of the reference algorithm) on `threads` host threads (0 = all): one
-    RK2 HLLD step of the n^3 grid; returns cell-updates/s, the thread count and the seconds."""
-    import numpy as np  # noqa: F401
+def cpu_baseline(n: int, tsteps_sample: int = 1, threads: int = 0, order: int = 2, scheme: int = 2,
+                 seed: int = 2, developed: bool = True):
+    """The oracle (CPU port of the reference algorithm) on `threads` host threads (0 = all):
+    `tsteps_sample` HLLD steps (minmod + Heun RK2 by default, or first order + forward Euler) of
+    the n^3 grid; returns cell-updates/s, the thread count and the seconds.  `developed` starts
+    from dt = 1e-4 instead of the reference's 2e-9 first step (the rate does not depend on dt)."""
     import oracle as O
     O.build()
     g = O.make_grid(n, r_floor=0.5 * 2.0 / n)
-    U = O.init_lism(g, seed=2)
+    U = O.init_lism(g, seed=seed)
     ck = O.clock_init(g)
-    ck.dt_next = 1e-4
+    if developed:
+        ck.dt_next = 1e-4
     threads = threads or O.max_threads()
     t0 = time.perf_counter()
-    O.run(g, O.make_opts(3, 2, 2, 0.4), U, tsteps_sample, ck, nthreads=threads)
+    O.run(g, O.make_opts(3, order, scheme, 0.4), U, tsteps_sample, ck, nthreads=threads)
     dt = time.perf_counter() - t0
     return n ** 3 * tsteps_sample / dt, threads, dt
+
+
+def cpu_baseline_line(n: int):
+    """The CPU baselines: the bench workload's grid (one RK2 step, all threads) as `value`, the
+    C2 parity grid (96^3, RK2) and config C1 (64^3, first order, forward Euler, 100 steps) at all
+    threads and one thread (bounded samples, ~15-25 s of CPU work in all)."""
+    v, thr, secs = cpu_baseline(n)
+    c2a, _, s2a = cpu_baseline(96, tsteps_sample=10)
+    c2b, _, s2b = cpu_baseline(96, tsteps_sample=1, threads=1)
+    c1a, _, s1a = cpu_baseline(64, tsteps_sample=100, order=1, scheme=1, seed=1, developed=False)
+    c1b, _, s1b = cpu_baseline(64, tsteps_sample=10, order=1, scheme=1, seed=1, developed=False, threads=1)
+    return {"value": v, "unit": "cell-updates/s", "cores": thr, "kind": "port",
+            "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid ({secs:.1f} s)",
+            "c2_96": {"all_threads": c2a, "cores": thr, "one_thread": c2b, "unit": "cell-updates/s",
+                      "sample": f"96^3 RK2 HLLD minmod: 10 steps on all threads ({s2a:.1f} s), 1 step on one "
+                                f"thread ({s2b:.1f} s)"},
+            "c1": {"all_threads": c1a, "cores": thr, "one_thread": c1b, "unit": "cell-updates/s",
+                   "sample": f"C1 64^3 first-order HLLD forward Euler: 100 steps on all threads ({s1a:.1f} s), "
+                             f"10 steps on one thread ({s1b:.1f} s)"}}
 
 
 def run_reference(args, world, rank):
@@ -157,16 +183,18 @@ def run_reference(args, world, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_dict(args, reference=True),
         "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid per bench step (of {args.tsteps} per solve)"},
+                         "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid per bench step, dt 1e-4 (the "
+                                   f"GPU arm's bench step is a {args.tsteps}-step solve; the metric is a rate)"},
         "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
 def config_dict(args, reference=False):
+    tps = 1 if reference else args.tsteps
     return {"workload": f"C2 plain FP64: ideal MHD, HLLD + minmod + Heun RK2, {args.n}^3 Cartesian, "
-                        f"{args.tsteps} time steps per bench step",
-            "grid": [args.n] * 3, "time_steps_per_step": args.tsteps, "n_state": 3, "order": 2, "scheme": "rk2",
+                        f"{tps} time step{'s' if tps > 1 else ''} per bench step",
+            "grid": [args.n] * 3, "time_steps_per_step": tps, "n_state": 3, "order": 2, "scheme": "rk2",
             "cfl": 0.4, "precision": "plain-fp64",
             "l2": "inputs larger than L2 (state 1.07 GB per buffer at 256^3)",
             "parallelism": f"replicas{args.gpus}" if args.gpus > 1 else "single"}
@@ -215,6 +243,48 @@ def run_mixed_only(args):
     print(json.dumps({"leg": f"mixed{args.mixed_precision}", "grid": n, "stage1_ms": ms[0] / max(cnt[0], 1),
                       "stage2_ms": ms[1] / max(cnt[1], 1),
                       "cell_updates_per_s": n ** 3 * T * args.steps / (sum(ms) / 1e3)}), flush=True)
+
+
+def run_c5(args):
+    """`--c5 K`: config C5 at its stated parameters on the first K requests of the seeded stream
+    (Poisson 20/s, cubic edges log-uniform [32,256], 30 % hydro / 70 % MHD, steady state when the
+    relative L1 change of rho between 50-step checks is below 1e-5, cap 3000 steps, CFL 0.2, 150 GB
+    admission budget), served in the mixed form by the native continuous-batching server, then the
+    same requests solved one at a time in the plain FP64 form.  Reports latency percentiles,
+    solves/s, convergence and failures, and the served-vs-plain L1 of rho for every request that
+    both ran to the same step count (states kept for edges <= 160 to bound host memory)."""
+    import numpy as np
+    import set_b200  # noqa: F401  (fails loudly without the CUDA library)
+    from set_b200 import workloads as WL, serve as SV
+    reqs = WL.c5_requests(count=args.c5, rate=20.0, lo=32, hi=256, max_steps=3000)
+    keep = [k for k, r in enumerate(reqs) if r.inst.desc.nx <= 160]
+    out = SV.run_stream(reqs, max_slots=256, precision=1, keep=keep)
+    t0 = time.perf_counter()
+    l1, same_steps, seq_steps, seq_conv = [], 0, [], 0
+    for k, rq in enumerate(reqs):
+        alone = SV.solve_alone(rq.inst, 0, rq.steady_tol, rq.max_steps, keep_state=k in out["states"])
+        seq_steps.append(alone["steps"])
+        seq_conv += int(alone["converged"])
+        if k in out["states"] and alone["steps"] == out["steps"][k] and out["results"][k].status == 0:
+            a, b = alone["U"][0], out["states"][k][0]
+            l1.append(float(np.abs(b - a).sum() / np.abs(a).sum()))
+            same_steps += 1
+    seq_secs = time.perf_counter() - t0
+    edges = [r.inst.desc.nx for r in reqs]
+    line = {"leg": "C5", "config": {"requests": len(reqs), "rate_per_s": 20.0, "edges": "cubic, log-uniform [32,256]",
+                                    "hydro_fraction": 0.3, "steady_tol": 1e-5, "check_every": 50, "max_steps": 3000,
+                                    "cfl": 0.2, "hbm_budget_bytes": 150 * 10 ** 9, "served_precision": "mixed",
+                                    "edge_min_max": [min(edges), max(edges)]},
+            "latency_p50_s": out["latency_p50_s"], "latency_p99_s": out["latency_p99_s"],
+            "solves_per_s": out["solves_per_s"], "span_s": out["span_s"], "max_active": out["max_active"],
+            "converged": out["converged"], "failed": out["failed"], "failed_by_status": out["failed_by_status"],
+            "steps_mean": float(np.mean(out["steps"])),
+            "sequential_plain_solves_per_s": len(reqs) / seq_secs, "sequential_plain_seconds": seq_secs,
+            "sequential_plain_converged": seq_conv,
+            "speedup_vs_sequential_plain": out["solves_per_s"] / (len(reqs) / seq_secs),
+            "l1_rho_served_vs_plain": {"compared": same_steps, "max": max(l1) if l1 else None,
+                                       "median": float(np.median(l1)) if l1 else None}}
+    print(json.dumps(line), flush=True)
 
 
 def run_slab(args, world, rank, local):
@@ -454,14 +524,19 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and args.facelist_n > 0:
         facelist = [facelist_leg(args.facelist_n, 50, False), facelist_leg(args.facelist_n, 50, True)]
 
+    # ---- config C3: one seeded Mach / beta draw at 384^3 x 500 steps, mixed against plain FP64
+    c3 = None
+    if rank == 0 and world == 1 and args.c3_n > 0:
+        from set_b200 import workloads as WL
+        r = WL.run_c3(WL.c3_problems(count=1, n=args.c3_n, steps=args.c3_steps), mixed=(1,))[0]
+        c3 = {"config": f"C3: {args.c3_n}^3, {args.c3_steps} steps, HLLD minmod Heun RK2, CFL 0.4, one seeded "
+                        f"draw of LISM Mach in [2,8] and beta in [0.1,10] ({r['label']})",
+              "plain_cell_updates_per_s": r["plain_cell_updates_per_s"], "mixed": r["mixed1"],
+              "plain_n_negdens": r["plain_n_negdens"]}
+
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, thr, secs = cpu_baseline(n)
-        v1, _, secs1 = cpu_baseline(64, threads=1)
-        base = {"value": v, "unit": "cell-updates/s", "cores": thr, "kind": "port",
-                "sample": f"1 RK2 HLLD minmod step of the {n}^3 grid ({secs:.1f} s)",
-                "single_thread": {"value": v1, "unit": "cell-updates/s", "cores": 1,
-                                  "sample": f"1 RK2 HLLD minmod step of the 64^3 grid ({secs1:.1f} s)"}}
+        base = cpu_baseline_line(n)
 
     if rank == 0:
         line = {
@@ -480,9 +555,9 @@ def run_ours(args, world, rank, local):
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
                          "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
                          "limiter": "FP64 latency and issue, not DRAM: at 160^3 ncu shows DRAM traffic 0.98x "
-                                    "algorithmic, FP64 pipe 40-42 %, issue 50-53 % at 12 warps/SM "
-                                    "(profiles/stage_plain_hlld_160cube.md)"},
+                                    "algorithmic, FP64 pipe 40-42 %, issue 50-53 % at 12 warps/SM"},
             "mixed": mixed,
+            "c3": c3,
             "ensemble": ensemble,
             "served": served,
             "facelist": facelist,
@@ -513,6 +588,11 @@ def main():
     ap.add_argument("--mixed-precision", type=int, default=1, choices=[1, 2],
                     help="mixed form: 1 FP32 Riemann arithmetic, 2 the delta form")
     ap.add_argument("--c3", type=int, default=0, help="run config C3 (mixed vs plain) on this many seeded draws")
+    ap.add_argument("--c3-n", type=int, default=384, help="C3 leg grid edge in the default line (0 = off)")
+    ap.add_argument("--c3-steps", type=int, default=500)
+    ap.add_argument("--c5", type=int, default=0,
+                    help="run config C5 at its stated parameters (edges [32,256], cap 3000 steps, steady state "
+                         "1e-5, 150 GB) on this many requests, served and sequential plain, and exit")
     ap.add_argument("--serve-requests", type=int, default=100)
     ap.add_argument("--facelist-n", type=int, default=128, help="face-list leg on an n^3 box (0 = off)")
     ap.add_argument("--serve-max-edge", type=int, default=96)
@@ -527,6 +607,8 @@ def main():
         run_mixed_only(args)
     elif args.decomp == "slab":
         run_slab(args, world, rank, local)
+    elif args.c5 > 0:
+        run_c5(args)
     elif args.c3 > 0:
         import set_b200  # noqa: F401  (fails loudly without the CUDA library)
         from set_b200 import workloads as WL

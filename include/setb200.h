@@ -200,6 +200,17 @@ SETB_API int32_t setb_get_conserved(setb_handle* h, double* U);
 /* Counters and clocks (replaces the reference's prints). Waits for the handle's stream. */
 SETB_API int32_t setb_status(setb_handle* h, setb_diag* out);
 
+/* No counterpart in the reference (its kernels have no device-side waits).  Sets how long the
+ * handle's stage kernels wait for a plane copy (the tensor copy that stages each z plane into
+ * shared memory) before they count the wait as run out: cycles > 0 is the limit in SM clock
+ * cycles, 0 restores the default (~2 s), cycles < 0 makes every wait a single non-blocking check
+ * (used by tests to drive the error path).  A wait that runs out is reported as SETB_ETIMEOUT by
+ * the next call that reads the counters (setb_step with time_all, setb_sync, setb_status); the
+ * kernel then gives the copy a second ~2 s wait before it reads the plane, and a copy that never
+ * lands switches that thread to plain loads, so the state stays valid.  setb_set_state clears the
+ * counters. */
+SETB_API int32_t setb_set_copy_wait(setb_handle* h, int64_t cycles);
+
 /* The CUDA stream the handle launches on (as a void* cudaStream_t). */
 SETB_API int32_t setb_stream(setb_handle* h, void** stream);
 
@@ -404,7 +415,9 @@ SETB_API int32_t setb_server_destroy(setb_server* s);
  * nx*ny*nz doubles with x fastest; it is advanced in place by nsteps steps of `o`.  *dt_io is the
  * dt of the first step on entry (desc->dt_init on a fresh run; desc->dt_init is not used) and the
  * dt of the next step on return; *time_io is the simulated time in and out; diag may be NULL.
- * Runs on `stream` (NULL: the legacy default stream) and waits for it before returning.
+ * Runs on `stream` (NULL: the legacy default stream) and is synchronous: it returns after the
+ * steps have finished and the clock and counters have been read back.  Arguments are checked as
+ * setb_init_cartesian and setb_step check them (precision must be 0).
  *
  * The scratch (the Heun stage buffer, the device clock, the error counters) is one fixed
  * file-scope device array of 16 MiB + 256 B that every GPU loading the library holds until the

@@ -104,6 +104,7 @@ _SIGS = {
     "setb_copy_state": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "setb_status": (C.c_int32, [C.c_void_p, C.POINTER(Diag)]),
     "setb_stream": (C.c_int32, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "setb_set_copy_wait": (C.c_int32, [C.c_void_p, C.c_int64]),
     "setb_init_slab": (C.c_int32, [C.POINTER(C.c_void_p), C.POINTER(CartDesc), C.c_int32, C.c_int32, _dp]),
     "setb_slab_stage": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(StepOpts)]),
     "setb_slab_view": (C.c_int32, [C.c_void_p, C.c_int32, C.POINTER(_dp), C.POINTER(C.c_int64),
@@ -400,6 +401,11 @@ class Solver:
     def copy_from(self, other: "Solver"):
         """Device-side copy of another handle's state, clock and counters (same grid)."""
         _check(lib().setb_copy_state(self.h, other.h), "setb_copy_state")
+
+    def set_copy_wait(self, cycles: int):
+        """Limit of the stage kernels' first wait on a plane copy (SM cycles; 0 = default ~2 s,
+        < 0 = one non-blocking check)."""
+        _check(lib().setb_set_copy_wait(self.h, int(cycles)), "setb_set_copy_wait")
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -42,6 +42,7 @@ struct setb_handle {
     FaceListDev* fl = nullptr;             // face-list grid (g is then 1-D: nx = N cells)
     int ctas_per_sm = 1;
     int sm_count = 148;
+    long long copy_wait = 0;               // StageArgs::copy_wait of this handle's launches
 };
 
 namespace {
@@ -52,7 +53,9 @@ namespace {
         if (e_ != cudaSuccess) return SETB_ECUDA;      \
     } while (0)
 
-int validate_desc(const setb_cart_desc* d) {
+}  // namespace
+
+int sb::validate_desc(const setb_cart_desc* d) {
     if (!d) return SETB_EINVAL;
     if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->flags != 0) return SETB_EINVAL;
     if ((long long)d->nx * d->ny * d->nz > (1ll << 31)) return SETB_ESIZE;
@@ -64,7 +67,7 @@ int validate_desc(const setb_cart_desc* d) {
     return SETB_OK;
 }
 
-int validate_opts(const setb_step_opts* o) {
+int sb::validate_opts(const setb_step_opts* o) {
     if (!o) return SETB_EINVAL;
     if (o->n_state < 0 || o->n_state > 3) return SETB_EINVAL;
     if (o->n_disc < 0 || o->n_disc > 2) return SETB_EINVAL;
@@ -76,6 +79,8 @@ int validate_opts(const setb_step_opts* o) {
     if (!(o->cfl > 0.0)) return SETB_EINVAL;
     return SETB_OK;
 }
+
+namespace {
 
 GridGeom make_geom(const setb_cart_desc* d) {
     GridGeom g{};
@@ -107,9 +112,11 @@ GridGeom make_geom(const setb_cart_desc* d) {
 constexpr int kShapeTy[2] = {tile_shape(0, 0).ty, tile_shape(1, 1).ty};
 int shape_index(int precision, int kind) { return tile_shape(precision, kind).ty == kShapeTy[0] ? 0 : 1; }
 
+}  // namespace
+
 // z extent of one CTA's march: balances wave quantisation against the per-chunk prologue
 // (4 plane loads + 1 z face, costed as ~1.5 plane iterations).
-int choose_lz(const GridGeom& g, int sm_count, int precision, int kind) {
+int sb::choose_lz(const GridGeom& g, int sm_count, int precision, int kind) {
     const TileShape ts = tile_shape(precision, kind);
     const long long cols = (long long)((g.nx + kTileX - 1) / kTileX) * ((g.ny + ts.ty - 1) / ts.ty);
     const long long slots = (long long)sm_count * std::max(ts.ctas_per_sm, 1);
@@ -128,6 +135,8 @@ int choose_lz(const GridGeom& g, int sm_count, int precision, int kind) {
     }
     return best_lz;
 }
+
+namespace {
 
 void clock_reset(setb_handle* h, double time_all) {
     DevClock c{};
@@ -614,6 +623,7 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     a.st = h->st;
     a.cfl = o->cfl;
     a.n_disc = o->n_disc;
+    a.copy_wait = h->copy_wait;
     const int shape0 = shape_index(P, 0), shape1 = shape_index(P, 1);
     if (ev) SB_TRY(cudaEventRecord(ev[0], h->stream));
     for (int s = 0; s < nsteps; s++) {
@@ -890,6 +900,7 @@ int32_t setb_slab_stage(setb_handle* h, int32_t stage, const setb_step_opts* o) 
     a.st = h->st;
     a.cfl = o->cfl;
     a.n_disc = o->n_disc;
+    a.copy_wait = h->copy_wait;
     a.Uin = X;
     a.tm_in = h->tma_ok[shape] ? h->tmap + 2 * in + shape : nullptr;
     if (stage == 1) {
@@ -905,6 +916,12 @@ int32_t setb_slab_stage(setb_handle* h, int32_t stage, const setb_step_opts* o) 
     }
     SB_TRY(launch_stage(a, P, o->n_state, o->order, kind, stage == 1, h->stream));
     if (stage == 1 && o->scheme == 1) h->cur = 1 - h->cur;
+    return SETB_OK;
+}
+
+int32_t setb_set_copy_wait(setb_handle* h, int64_t cycles) {
+    if (!h) return SETB_EINVAL;
+    h->copy_wait = cycles;
     return SETB_OK;
 }
 

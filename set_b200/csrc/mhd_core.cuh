@@ -93,11 +93,15 @@ SB_HD float sb_rsqrt(float x) {
 // the FP64 approximate instructions (relative error ~1e-6, measured) refined by Newton-Raphson
 // iteration -- two steps y <- y + y (1 - x y) for 1/x, two steps y <- y + (y/2)(1 - x y^2) for
 // 1/sqrt(x) -- and sqrt(x) as x y after one such step, corrected by one step of Heron's method
-// s <- s + (y/2)(x - s^2).  Measured on 2^20 inputs spanning 1e-9..1e9: 1/x and sqrt(x) correctly
-// rounded, 1/sqrt(x) within 1 ulp.  These dependent fused multiply-adds are a shorter chain than
-// the correctly rounded library forms, which the FP64 flux's latency-bound schedule rewards; the
-// state conversions and the mixed form keep the library forms (there the Newton forms measured
-// slower).  On the host all three are the IEEE operations.
+// s <- s + (y/2)(x - s^2).  Domain: positive normal x whose result is normal (the approximate
+// instructions flush subnormals); there 1/x and sqrt(x) are correctly rounded and 1/sqrt(x) is
+// within 1 ulp (tests/test_gpu_special.py checks 2^20 inputs over 1e-300..1e300).  At 0, +-inf
+// and subnormals 1/x and 1/sqrt(x) give NaN (sqrt(0) = 0); the plain stage kernel recomputes a
+// face whose energy flux is non-finite with the library forms.  These dependent fused
+// multiply-adds are a shorter chain than the correctly rounded library forms, which the FP64
+// flux's latency-bound schedule rewards; the state conversions and the mixed form keep the
+// library forms (there the Newton forms measured slower).  On the host all three are the IEEE
+// operations.
 SB_HD double rs_rcp(double x) {
 #if defined(__CUDA_ARCH__)
     double y;
@@ -146,6 +150,15 @@ template <bool NR, typename T> SB_HD T fr_rsqrt(T x) {
 template <bool NR, typename T> SB_HD T fr_sqrt(T x) {
     if constexpr (NR) return rs_sqrt(x);
     else return sb_sqrt(x);
+}
+
+// false for +-inf and NaN (an exponent test on the high word: no FP64 instruction).
+SB_HD bool sb_isfinite(double x) {
+#if defined(__CUDA_ARCH__)
+    return (__double2hiint(x) & 0x7ff00000) != 0x7ff00000;
+#else
+    return std::isfinite(x);
+#endif
 }
 
 template <typename T> SB_HD T sb_abs(T x) { return x < T(0) ? -x : x; }

@@ -76,20 +76,24 @@ extern "C" int32_t setb_step_noalloc(const setb_cart_desc* d, const setb_step_op
                                      int64_t var_stride, int32_t nsteps, double* dt_io, double* time_io,
                                      setb_diag* diag, void* stream) {
     if (!d || !o || !U || !dt_io || !time_io || nsteps < 0) return SETB_EINVAL;
-    if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->flags != 0) return SETB_EINVAL;
+    // the same checks as setb_init_cartesian / setb_step, with the first dt taken from *dt_io
+    setb_cart_desc dd = *d;
+    dd.dt_init = *dt_io;
+    int rc = validate_desc(&dd);
+    if (rc == SETB_OK) rc = validate_opts(o);
+    if (rc) return rc;
+    if (o->precision != 0) return SETB_EINVAL;   // plain FP64 only: no compensation array
     const long long N = (long long)d->nx * d->ny * d->nz;
     if (N > kNoAllocMaxCells || var_stride > kNoAllocMaxCells) return SETB_ESIZE;
     if (var_stride < N) return SETB_EINVAL;
-    if (o->n_state < 0 || o->n_state > 3 || o->n_disc < 0 || o->n_disc > 2 || (o->order != 1 && o->order != 2) ||
-        (o->scheme != 1 && o->scheme != 2) || o->precision != 0 || o->reserved != 0 || !(o->cfl > 0.0))
-        return SETB_EINVAL;
-    if (!(*dt_io > 0.0)) return SETB_EINVAL;
-    for (int a = 0; a < 3; a++)
-        if (!(d->hi[a] > d->lo[a])) return SETB_EINVAL;
 
     double* scratch = nullptr;
-    int rc = scratch_for_current_device(&scratch);
+    rc = scratch_for_current_device(&scratch);
     if (rc) return rc;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        return SETB_ECUDA;
     DevClock* clk = reinterpret_cast<DevClock*>(scratch);
     DevStatus* st = reinterpret_cast<DevStatus*>(reinterpret_cast<char*>(scratch) + sizeof(DevClock));
     double* W = scratch + kHeaderDoubles;   // U*: 8 planes at the caller's var_stride
@@ -118,7 +122,7 @@ extern "C" int32_t setb_step_noalloc(const setb_cart_desc* d, const setb_step_op
     a.g.v_src = d->v_src;
     a.g.p_over_rho_src = d->p_over_rho_src;
     a.g.r_floor = d->r_floor;
-    a.g.lz = d->nz;   // small grids: one march per column tile
+    a.g.lz = choose_lz(a.g, sms, 0, 0);   // the handle path's z chunking (same tiles, same faces)
     a.clk = clk;
     a.st = st;
     a.cfl = o->cfl;
@@ -179,6 +183,7 @@ extern "C" int32_t setb_step_noalloc(const setb_cart_desc* d, const setb_step_op
         diag->n_recon_err = (int64_t)st_h.n_recon;
         diag->n_fp64_redo = (int64_t)st_h.n_redo;
     }
+    if (st_h.n_timeout) return SETB_ETIMEOUT;
     if (st_h.n_negdens) return SETB_ENEGDENS;
     if (st_h.n_wave) return SETB_EWAVES;
     if (st_h.n_recon) return SETB_ERECON;

@@ -98,7 +98,21 @@ struct StageArgs {
     const CUtensorMap* tm_in;           // tensor map of Uin (device memory) for the plane
                                         // copies, box (kTileX + 4, ty + 4, 1, 8) of this form's
                                         // tile; null = planes read with plain loads
+    long long copy_wait;                // limit of the first wait for a plane copy, in SM cycles:
+                                        // 0 = kCopyWaitCycles, < 0 = one non-blocking check
+                                        // (setb_set_copy_wait; tests of the timeout path)
 };
+
+// Default limit of a bounded wait on a plane copy (~2 s at 1.965 GHz), and of the second wait
+// that lets a late copy land after the first one ran out.
+constexpr long long kCopyWaitCycles = 4000000000ll;
+
+// Host-side argument checks shared by every entry point that takes a grid or scheme options
+// (capi.cu): SETB_OK or the status to return.
+int validate_desc(const setb_cart_desc* d);
+int validate_opts(const setb_step_opts* o);
+// z extent of one CTA's march for a grid on sm_count SMs (capi.cu).
+int choose_lz(const GridGeom& g, int sm_count, int precision, int kind);
 
 // One launch of the batch kernel: tiles of many solves behind one work-queue counter.
 struct BatchArgs {

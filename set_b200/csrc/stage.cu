@@ -23,6 +23,7 @@
 //   the Euler step) is a compensated sum with the compensation kept in FP32; dt is reduced in
 //   FP64.  Half the shared memory and at most 128 registers give two CTAs per SM.
 // P = 2, delta form: FP64 ring and fluxes, the Riemann solver's small differences in FP32.
+#include <atomic>
 #include <cfloat>
 #include <type_traits>
 #include "riemann_f32x2.cuh"
@@ -104,12 +105,26 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
     return ok != 0;
 }
 
-// Waits for phase `parity` of the barrier, for at most ~2 s of SM clock; false when it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+// Non-blocking probe of phase `parity` of the barrier.
+__device__ __forceinline__ bool mbar_test_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for phase `parity` of the barrier for at most `limit` SM cycles (0: kCopyWaitCycles,
+// < 0: one non-blocking check); false when it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, long long limit) {
+    if (limit < 0) return mbar_test_wait(bar, parity);
+    if (limit == 0) limit = kCopyWaitCycles;
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > 4000000000ll) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -236,9 +251,12 @@ __device__ __noinline__ int face_fp64_states(const double* q1, const double* q2,
     return riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, n_disc, F, *sl, *sr, SM);
 }
 
+// `n_waits` counts the completed phases of `bar` and `tma_dead` is set once a plane copy did not
+// land within both bounded waits (the thread then reads its planes with plain loads); both are
+// per thread and carried across the tiles a CTA runs.
 template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT, int SK>
 __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int bz, unsigned total_tiles,
-                                         unsigned long long* bar, unsigned& n_waits) {
+                                         unsigned long long* bar, unsigned& n_waits, bool& tma_dead) {
     using RG = typename Types<P>::Ring;
     using FT = typename Types<P>::Flux;
     using RT = typename Types<P>::Math;
@@ -252,7 +270,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     FT* fx = reinterpret_cast<FT*>(ring + RING * 8 * PLANE);   // [8][NXF]
     FT* fy = fx + 8 * NXF;                                      // [8][NYF]
     __shared__ double red[NT / 32];
-    __shared__ unsigned long long cnt[5];
+    __shared__ unsigned long long cnt[6];
     __shared__ bool last_cta;
 
     const GridGeom& g = A.g;
@@ -263,10 +281,10 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     const int k0 = kb + bz * g.lz;
     const int k1 = min(ke, k0 + g.lz);
     const double dt = A.clk->dt_cur;
-    if (t < 5) cnt[t] = 0;
+    if (t < 6) cnt[t] = 0;
 
     double rate = 0.0;   // max over this thread's real faces of max(|SL|,|SR|)/dist
-    unsigned n_recon = 0, n_wave = 0, n_redo = 0;
+    unsigned n_recon = 0, n_wave = 0, n_redo = 0, n_tmo = 0;
 
     // Faces are handed out in warp-sized jobs, so the face axis is uniform across a warp and the
     // face-frame permutation of the components is a compile-time constant of the gather and the
@@ -365,10 +383,14 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             sr = (double)SR;
         }
         const double sq = g.square[axis];
-        if (P == 1 && real && (fl & kFlagStar)) {
+        // The plain form's Newton-refined special functions (rs_rcp & co.) are defined on normal
+        // finite arguments; a face whose energy flux comes out non-finite is recomputed with the
+        // IEEE library forms, out of line (a state that is already invalid stays invalid).
+        const bool redo64 = real && ((P == 1 && (fl & kFlagStar)) || (P == 0 && !sb_isfinite((double)F[4])));
+        if (redo64) {
             double F64[8];
             fl = face_fp64<NSTATE, ORDER>(A, axis, i0 + fxx, j0 + fyy, gk, F64, &sl, &sr);
-            if (!dup) n_redo++;
+            if (!dup && P == 1) n_redo++;
 #pragma unroll
             for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (FT)(F64[v] * sq);
         } else {
@@ -390,7 +412,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     // update).  Every face goes through the one do_face call site below, so a face's arithmetic
     // does not depend on where a chunk starts.  With a tensor map, the copy of plane kk+1 is in
     // flight while plane kk's faces and updates run; the last copy issued is plane k1+1.
-    const bool use_tma = A.tm_in != nullptr;
+    const bool use_tma = A.tm_in != nullptr && !tma_dead;
     constexpr unsigned kPlaneBytes = 8u * PLANE * sizeof(double);
     const int kz_last = k1 + 1;
     auto issue_copy = [&](int kk) {
@@ -407,15 +429,22 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     const bool own = (t < NC) && (gi < g.nx) && (gj < g.ny);
     for (int kk = k0 - 2; kk <= kz_last; kk++) {
         RG* slot = ring + ring_slot(kk) * 8 * PLANE;
-        if (use_tma) {
-            if (!mbar_wait_bounded(bar, n_waits & 1u)) atomicAdd(&A.st->n_timeout, 1ull);
+        if (use_tma && !tma_dead) {
+            // A wait that runs out is counted (SETB_ETIMEOUT), then the copy gets a second bounded
+            // wait to land before the box is read; a copy that never lands switches this thread to
+            // plain loads (and thread 0 stops issuing copies), so no read races a late copy.
+            bool ok = mbar_wait_bounded(bar, n_waits & 1u, A.copy_wait);
+            if (!ok) {
+                n_tmo++;
+                ok = mbar_wait_bounded(bar, n_waits & 1u, kCopyWaitCycles);
+            }
             n_waits++;
-            convert_plane<P, SK, RG>(A, stg, slot, i0, j0);
-        } else {
-            load_plane<P, SK, RG>(A, slot, i0, j0, kk);
+            if (ok) convert_plane<P, SK, RG>(A, stg, slot, i0, j0);
+            else tma_dead = true;
         }
+        if (!use_tma || tma_dead) load_plane<P, SK, RG>(A, slot, i0, j0, kk);
         __syncthreads();
-        if (use_tma && t == 0 && kk < kz_last) issue_copy(kk + 1);
+        if (use_tma && !tma_dead && t == 0 && kk < kz_last) issue_copy(kk + 1);
         const int k = kk - 2;
         if (k < k0 - 1) continue;
         const bool pro = (k < k0);
@@ -513,6 +542,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     if (n_recon) atomicAdd(&cnt[2], (unsigned long long)n_recon);
     if (n_wave) atomicAdd(&cnt[3], (unsigned long long)n_wave);
     if (n_redo) atomicAdd(&cnt[4], (unsigned long long)n_redo);
+    if (n_tmo) atomicAdd(&cnt[5], (unsigned long long)n_tmo);
     if (WANT_DT) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, o));
@@ -532,6 +562,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         if (cnt[2]) atomicAdd(&A.st->n_recon, cnt[2]);
         if (cnt[3]) atomicAdd(&A.st->n_wave, cnt[3]);
         if (cnt[4]) atomicAdd(&A.st->n_redo, cnt[4]);
+        if (cnt[5]) atomicAdd(&A.st->n_timeout, cnt[5]);
         __threadfence();
         const unsigned ticket = atomicAdd(&A.clk->counter, 1u);
         last_cta = (ticket == total_tiles - 1);
@@ -559,8 +590,9 @@ __global__ void __launch_bounds__(Tile<P, KIND>::NT, Tile<P, KIND>::MINB) stage_
     if (threadIdx.x == 0) mbar_init(&bar);
     __syncthreads();
     unsigned n_waits = 0;
+    bool tma_dead = false;
     run_tile<P, NSTATE, ORDER, KIND, WANT_DT, KIND>(A, blockIdx.x, blockIdx.y, blockIdx.z,
-                                                     gridDim.x * gridDim.y * gridDim.z, &bar, n_waits);
+                                                     gridDim.x * gridDim.y * gridDim.z, &bar, n_waits, tma_dead);
 }
 
 // Persistent batch kernel: each CTA takes tiles from the work queue until it is empty; the
@@ -575,6 +607,7 @@ __global__ void __launch_bounds__(Tile<P, kBatchKind>::NT, Tile<P, kBatchKind>::
     static_assert(sizeof(StageArgs) % sizeof(unsigned long long) == 0, "StageArgs must be 8-byte granular");
     if (threadIdx.x == 0) mbar_init(&bar);
     unsigned n_waits = 0;   // completed phases of `bar`, the same count in every thread
+    bool tma_dead = false;
     for (;;) {
         if (threadIdx.x == 0) {
             const unsigned i = atomicAdd(B.queue, 1u);
@@ -588,9 +621,9 @@ __global__ void __launch_bounds__(Tile<P, kBatchKind>::NT, Tile<P, kBatchKind>::
         for (int q = threadIdx.x; q < WORDS; q += Tile<P, kBatchKind>::NT) dst[q] = src[q];
         __syncthreads();
         if (As.n_state == 3)
-            run_tile<P, 3, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
+            run_tile<P, 3, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits, tma_dead);
         else
-            run_tile<P, 2, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits);
+            run_tile<P, 2, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits, tma_dead);
     }
 }
 
@@ -606,11 +639,18 @@ template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
     auto kern = stage_kernel<P, NSTATE, ORDER, KIND, WANT_DT>;
     const int smem = smem_bytes<P, KIND>();
-    static bool attr_set = false;   // per process; every device shares the same limit
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // The dynamic shared-memory opt-in is a per-device attribute of the kernel: set it once per
+    // device ordinal (a bit per device, atomically; two threads that both set it set the same
+    // value), and on every launch for ordinals beyond the mask.
+    static std::atomic<unsigned long long> attr_set{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (!bit || !(attr_set.load(std::memory_order_acquire) & bit)) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        attr_set.fetch_or(bit, std::memory_order_release);
     }
     constexpr int TX = Tile<P, KIND>::TX, TY = Tile<P, KIND>::TY;
     const int nzu = plane_end(a.g) - plane_begin(a.g);

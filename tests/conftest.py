@@ -29,3 +29,11 @@ def has_gpu() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def gpu_count() -> int:
+    try:
+        import torch
+        return torch.cuda.device_count() if torch.cuda.is_available() else 0
+    except Exception:
+        return 0

@@ -1,0 +1,75 @@
+"""The plain form's FP64 special functions on the device (set_b200/csrc/mhd_core.cuh: rs_rcp,
+rs_rsqrt, rs_sqrt: Newton-refined approximate instructions) against IEEE results.
+
+tests/csrc/rs_special.cu wraps them in a kernel; this test compiles it with nvcc for sm_100a
+into a temporary library.  The reference values are numpy's correctly rounded 1/x and sqrt(x),
+and 1/sqrt(x) evaluated in extended precision and rounded once.
+"""
+import ctypes as C
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(os.path.dirname(HERE), "set_b200", "csrc")
+
+
+@pytest.fixture(scope="module")
+def rs_lib(tmp_path_factory):
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    nvcc = nvcc if os.path.exists(nvcc) else shutil.which("nvcc")
+    out = str(tmp_path_factory.mktemp("rs") / "librs.so")
+    subprocess.check_call([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                           "-Xcompiler", "-fPIC", "-shared", "-I" + CSRC,
+                           os.path.join(HERE, "csrc", "rs_special.cu"), "-o", out])
+    lib = C.CDLL(out)
+    lib.rs_eval.restype = C.c_int
+    lib.rs_eval.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_longlong]
+    return lib
+
+
+def rs_eval(lib, x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros((x.size, 3))
+    rc = lib.rs_eval(x.ctypes.data_as(C.POINTER(C.c_double)), out.ctypes.data_as(C.POINTER(C.c_double)), x.size)
+    assert rc == 0
+    return out
+
+
+def ulps(a, b):
+    """Distance in units in the last place between doubles of the same sign."""
+    ia = a.view(np.int64)
+    ib = b.view(np.int64)
+    return np.abs(ia - ib)
+
+
+def test_special_functions_on_their_domain(rs_lib):
+    rng = np.random.default_rng(1)
+    x = 10.0 ** rng.uniform(-300.0, 300.0, 1 << 20)
+    r = rs_eval(rs_lib, x)
+    rcp_ref = 1.0 / x
+    sqrt_ref = np.sqrt(x)
+    rsq_ref = (np.longdouble(1.0) / np.sqrt(x.astype(np.longdouble))).astype(np.float64)
+    d_rcp, d_rsq, d_sqrt = ulps(r[:, 0], rcp_ref), ulps(r[:, 1], rsq_ref), ulps(r[:, 2], sqrt_ref)
+    assert d_rcp.max() <= 1 and d_rsq.max() <= 1 and d_sqrt.max() <= 1, (d_rcp.max(), d_rsq.max(), d_sqrt.max())
+    # 1/x and sqrt(x) correctly rounded on (almost) every input; 1/sqrt(x) within 1 ulp
+    assert (d_rcp == 0).mean() >= 0.9999, (d_rcp == 0).mean()
+    assert (d_sqrt == 0).mean() >= 0.9999, (d_sqrt == 0).mean()
+    # negative arguments of the reciprocal (SL - SM < 0 in the flux)
+    rn = rs_eval(rs_lib, -x[:4096])
+    assert ulps(-rn[:, 0], rcp_ref[:4096]).max() <= 1
+
+
+def test_special_functions_outside_their_domain(rs_lib):
+    """The documented edge behaviour: sqrt(0) = 0; 1/x and 1/sqrt(x) are NaN at 0, inf and
+    subnormals (the approximate instructions flush subnormals).  The stage kernel recomputes a
+    face whose energy flux is non-finite with the IEEE library forms."""
+    edge = np.array([0.0, np.inf, 5e-324, 1e-310])
+    r = rs_eval(rs_lib, edge)
+    assert r[0, 2] == 0.0
+    assert np.isnan(r[:, 0]).all() and np.isnan(r[:, 1]).all()
