@@ -96,8 +96,11 @@ SB_HD float sb_rsqrt(float x) {
 // s <- s + (y/2)(x - s^2).  Domain: positive normal x whose result is normal (the approximate
 // instructions flush subnormals); there 1/x and sqrt(x) are correctly rounded and 1/sqrt(x) is
 // within 1 ulp (tests/test_gpu_special.py checks 2^20 inputs over 1e-300..1e300).  At 0, +-inf
-// and subnormals 1/x and 1/sqrt(x) give NaN (sqrt(0) = 0); the plain stage kernel recomputes a
-// face whose energy flux is non-finite with the library forms.  These dependent fused
+// and subnormals 1/x and 1/sqrt(x) give NaN (sqrt(0) = 0).  Every argument the flux passes them
+// is a positive density, a sum of squares under sb_pos, or a wave-speed difference that a valid
+// state keeps away from zero (SR - SL >= cfL + cfR > 0; the star denominators tt are screened
+// against 1e-9 before the reciprocal); a state that is already invalid (rho <= 0) is reported by
+// the cell update's counters either way.  These dependent fused
 // multiply-adds are a shorter chain than the correctly rounded library forms, which the FP64
 // flux's latency-bound schedule rewards; the state conversions and the mixed form keep the
 // library forms (there the Newton forms measured slower).  On the host all three are the IEEE
@@ -150,15 +153,6 @@ template <bool NR, typename T> SB_HD T fr_rsqrt(T x) {
 template <bool NR, typename T> SB_HD T fr_sqrt(T x) {
     if constexpr (NR) return rs_sqrt(x);
     else return sb_sqrt(x);
-}
-
-// false for +-inf and NaN (an exponent test on the high word: no FP64 instruction).
-SB_HD bool sb_isfinite(double x) {
-#if defined(__CUDA_ARCH__)
-    return (__double2hiint(x) & 0x7ff00000) != 0x7ff00000;
-#else
-    return std::isfinite(x);
-#endif
 }
 
 template <typename T> SB_HD T sb_abs(T x) { return x < T(0) ? -x : x; }

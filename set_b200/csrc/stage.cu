@@ -175,6 +175,11 @@ template <int AX> __host__ __device__ constexpr int face_perm(int v) {
            : (v < 4 ? 0 : 4) + ((v & 3) == 1 ? 1 + AX : ((v & 3) == 2 ? (AX == 0 ? 2 : 1) : (AX == 2 ? 2 : 3)));
 }
 
+// face_perm<AX>(v) for an axis known only at run time (the rare FP64 recompute path).
+__device__ __forceinline__ int face_perm_dyn(int axis, int v) {
+    return axis == 0 ? face_perm<0>(v) : (axis == 1 ? face_perm<1>(v) : face_perm<2>(v));
+}
+
 // Face-frame states of the 4-cell stencil of a face normal to AX, from ring cells (component
 // planes PLANE apart).  B is first order, so only the inner pair carries it.
 template <int AX, int PLANE, typename RG, typename RT>
@@ -197,17 +202,65 @@ __device__ __forceinline__ void scatter_face(FT* out, const RT* F, RT sq) {
     for (int v = 0; v < 8; v++) out[face_perm<AX>(v) * STRIDE] = (FT)(F[v] * sq);
 }
 
-// The FP64 recompute of one face of the mixed form (rare path; kept out of line so the FP32
-// path keeps its registers).  (i, j, k) is the cell on the high side of the face.
+// What the out-of-line FP64 recompute of a face needs, passed by value: a reference or pointer to
+// the kernel's arguments would make the compiler copy them to local memory and read every field
+// from there on the hot path.
+struct FetchArgs {
+    const double* Uin;
+    long long vs, ps, px;
+    int nx, ny, nz, n_disc;
+    double inflow[8];
+};
+struct FaceFlux {
+    double F[8];   // natural component order
+    double sl, sr;
+    int fl;
+};
+
+__device__ __forceinline__ FetchArgs fetch_args(const StageArgs& A) {
+    FetchArgs f;
+    f.Uin = A.Uin;
+    f.vs = A.g.vs;
+    f.ps = A.g.ps;
+    f.px = A.g.px;
+    f.nx = A.g.nx;
+    f.ny = A.g.ny;
+    f.nz = A.g.nz;
+    f.n_disc = A.n_disc;
+#pragma unroll
+    for (int v = 0; v < 8; v++) f.inflow[v] = A.g.inflow[v];
+    return f;
+}
+
+// FP64 primitive state of global cell (i,j,k), boundary rules as fetch_prim64.
+__device__ __forceinline__ void fetch_prim64_f(const FetchArgs& f, int i, int j, int k, double* q) {
+    if (i >= f.nx) {
+#pragma unroll
+        for (int v = 0; v < 8; v++) q[v] = f.inflow[v];
+        return;
+    }
+    i = max(i, 0);
+    j = min(max(j, 0), f.ny - 1);
+    k = min(max(k, 0), f.nz - 1);
+    const long long off = (long long)k * f.ps + (long long)j * f.px + i;
+    double U[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) U[v] = __ldg(f.Uin + v * f.vs + off);
+    double ke, me;
+    prim_from_cons(U, q, ke, me);
+}
+
+// The FP64 recompute of one face of the mixed and delta forms from the FP64 state (rare path;
+// kept out of line so the main path keeps its registers), with the library special functions.
+// (i, j, k) is the cell on the high side of the face.
 template <int NSTATE, int ORDER>
-__device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j, int k, double* F, double* sl,
-                                      double* sr) {
+__device__ __noinline__ FaceFlux face_fp64(const FetchArgs fa, int axis, int i, int j, int k) {
     const int di = axis == 0, dj = axis == 1, dk = axis == 2;
     double c[4][8];
-    fetch_prim64(A, i - 2 * di, j - 2 * dj, k - 2 * dk, c[0]);
-    fetch_prim64(A, i - di, j - dj, k - dk, c[1]);
-    fetch_prim64(A, i, j, k, c[2]);
-    fetch_prim64(A, i + di, j + dj, k + dk, c[3]);
+    fetch_prim64_f(fa, i - 2 * di, j - 2 * dj, k - 2 * dk, c[0]);
+    fetch_prim64_f(fa, i - di, j - dj, k - dk, c[1]);
+    fetch_prim64_f(fa, i, j, k, c[2]);
+    fetch_prim64_f(fa, i + di, j + dj, k + dk, c[3]);
     const int pn = 1 + axis, pt1 = axis == 0 ? 2 : 1, pt2 = axis == 2 ? 2 : 3;
     const int perm[8] = {0, pn, pt1, pt2, 4, 4 + pn, 4 + pt1, 4 + pt2};
     double f[4][8];
@@ -215,9 +268,10 @@ __device__ __noinline__ int face_fp64(const StageArgs& A, int axis, int i, int j
         for (int v = 0; v < 8; v++) f[s][v] = c[s][perm[v]];
     double q1[8], q2[8], G[8], SM;
     reconstruct<double, ORDER>(f[0], f[1], f[2], f[3], q1, q2);
-    const int fl = riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, A.n_disc, G, *sl, *sr, SM);
-    for (int v = 0; v < 8; v++) F[perm[v]] = G[v];
-    return fl;
+    FaceFlux r;
+    r.fl = riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, fa.n_disc, G, r.sl, r.sr, SM);
+    for (int v = 0; v < 8; v++) r.F[perm[v]] = G[v];
+    return r;
 }
 
 // One tile of one stage: the column (bx, by) of TX x TY cells, planes [bz*lz, min(nz, (bz+1)*lz)).
@@ -241,15 +295,6 @@ template <> struct Types<1> {
     using Flux = float;
     using Math = float;
 };
-
-// FP64 recompute of a face of the delta form from its (FP64) face states; out of line so the
-// main path keeps its registers.
-template <int NSTATE>
-__device__ __noinline__ int face_fp64_states(const double* q1, const double* q2, int n_disc, double* F, double* sl,
-                                             double* sr) {
-    double SM;
-    return riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, n_disc, F, *sl, *sr, SM);
-}
 
 // `n_waits` counts the completed phases of `bar` and `tma_dead` is set once a plane copy did not
 // land within both bounded waits (the thread then reads its planes with plain loads); both are
@@ -365,8 +410,13 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             fl = riemann_delta<NSTATE>(q1, q2, F, SLf, SRf, SMf);
             sl = (double)SLf;
             sr = (double)SRf;
-            if (fl & kFlagStar) {
-                fl = face_fp64_states<NSTATE>(q1, q2, A.n_disc, F, &sl, &sr);
+            if (fl & kFlagStar) {   // the same face states, refetched: FP64 throughout
+                const FaceFlux r = face_fp64<NSTATE, ORDER>(fetch_args(A), axis, i0 + fxx, j0 + fyy, gk);
+                fl = r.fl;
+                sl = r.sl;
+                sr = r.sr;
+#pragma unroll
+                for (int v = 0; v < 8; v++) F[v] = r.F[face_perm_dyn(axis, v)];
                 if (real && !dup) n_redo++;
             }
         } else {
@@ -383,16 +433,14 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             sr = (double)SR;
         }
         const double sq = g.square[axis];
-        // The plain form's Newton-refined special functions (rs_rcp & co.) are defined on normal
-        // finite arguments; a face whose energy flux comes out non-finite is recomputed with the
-        // IEEE library forms, out of line (a state that is already invalid stays invalid).
-        const bool redo64 = real && ((P == 1 && (fl & kFlagStar)) || (P == 0 && !sb_isfinite((double)F[4])));
-        if (redo64) {
-            double F64[8];
-            fl = face_fp64<NSTATE, ORDER>(A, axis, i0 + fxx, j0 + fyy, gk, F64, &sl, &sr);
-            if (!dup && P == 1) n_redo++;
+        if (P == 1 && real && (fl & kFlagStar)) {
+            const FaceFlux r = face_fp64<NSTATE, ORDER>(fetch_args(A), axis, i0 + fxx, j0 + fyy, gk);
+            fl = r.fl;
+            sl = r.sl;
+            sr = r.sr;
+            if (!dup) n_redo++;
 #pragma unroll
-            for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (FT)(F64[v] * sq);
+            for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (FT)(r.F[v] * sq);
         } else {
             if (fl & kFlagWave) {
 #pragma unroll
@@ -419,7 +467,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         tma_plane(stg, A.tm_in, i0 - 2, j0 - 2, min(max(kk, 0), g.nz - 1), kPlaneBytes, bar);
     };
     if (use_tma && t == 0) issue_copy(k0 - 2);
-    double fzl[8];   // z fluxes k-1/2 (carried) and k+1/2 of this thread's column
+    FT fzl[8];       // z fluxes k-1/2 (carried) and k+1/2 of this thread's column
     // centre of this thread's column and its part of the source-sphere test
     const double cxs = cell_coord(g.lo[0], i0 + tx, g.h[0]), cys = cell_coord(g.lo[1], j0 + ty, g.h[1]);
     const double xy2 = dadd(dmul(cxs, cxs), dmul(cys, cys));
@@ -450,11 +498,11 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         const bool pro = (k < k0);
         const int njobs = pro ? JZ : JOBS;
         for (int job = warp; job < njobs; job += NW) do_face(job, k, pro && k0 > kb);
-        double fzh[8];
+        FT fzh[8];
         {
             const RG* zk = ring + ring_slot(k - 1) * 8 * PLANE + (ty + 2) * HX + tx + 2;
 #pragma unroll
-            for (int v = 0; v < 8; v++) fzh[v] = t < NC ? (double)zk[v * PLANE] : 0.0;
+            for (int v = 0; v < 8; v++) fzh[v] = t < NC ? zk[v * PLANE] : FT(0);
         }
         __syncthreads();
         if (pro) {
@@ -482,13 +530,24 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                 double uin[8], cmp[8];
 #pragma unroll
                 for (int v = 0; v < 8; v++) {
-                    double pot = 0.0;
-                    pot = pot - (double)fx[v * NXF + ty * (TX + 1) + tx];
-                    pot = pot + (double)fx[v * NXF + ty * (TX + 1) + tx + 1];
-                    pot = pot - (double)fy[v * NYF + ty * TX + tx];
-                    pot = pot + (double)fy[v * NYF + (ty + 1) * TX + tx];
-                    pot = pot - fzl[v];
-                    pot = pot + fzh[v];
+                    double pot;
+                    if constexpr (P == 1) {
+                        // FP32 fluxes: each opposite-face difference is exact when the two fluxes
+                        // are within a factor 2 (Sterbenz) and otherwise rounds relative to the
+                        // difference, far below the fluxes' own FP32 rounding; one conversion
+                        // per variable instead of six
+                        const float ax = fx[v * NXF + ty * (TX + 1) + tx + 1] - fx[v * NXF + ty * (TX + 1) + tx];
+                        const float ay = fy[v * NYF + (ty + 1) * TX + tx] - fy[v * NYF + ty * TX + tx];
+                        pot = (double)((ax + ay) + (fzh[v] - fzl[v]));
+                    } else {
+                        pot = 0.0;
+                        pot = pot - (double)fx[v * NXF + ty * (TX + 1) + tx];
+                        pot = pot + (double)fx[v * NXF + ty * (TX + 1) + tx + 1];
+                        pot = pot - (double)fy[v * NYF + ty * TX + tx];
+                        pot = pot + (double)fy[v * NYF + (ty + 1) * TX + tx];
+                        pot = pot - (double)fzl[v];
+                        pot = pot + (double)fzh[v];
+                    }
                     uin[v] = A.Uin[v * g.vs + off];
                     const double inc = dt * (pot * g.inv_vol);
                     if (P != 0 && A.comp) {

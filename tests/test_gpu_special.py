@@ -67,8 +67,8 @@ def test_special_functions_on_their_domain(rs_lib):
 
 def test_special_functions_outside_their_domain(rs_lib):
     """The documented edge behaviour: sqrt(0) = 0; 1/x and 1/sqrt(x) are NaN at 0, inf and
-    subnormals (the approximate instructions flush subnormals).  The stage kernel recomputes a
-    face whose energy flux is non-finite with the IEEE library forms."""
+    subnormals (the approximate instructions flush subnormals).  The flux never passes them such
+    arguments from a valid state."""
     edge = np.array([0.0, np.inf, 5e-324, 1e-310])
     r = rs_eval(rs_lib, edge)
     assert r[0, 2] == 0.0
