@@ -5,9 +5,10 @@
 //   compensation, a density snapshot for steady-state checks) allocated stream-ordered on the
 //   batch stream, so admitting or retiring a solve never synchronises the device.  Admission is
 //   by HBM footprint against a byte budget.
-// * A step is two persistent launches (Heun stages) whose CTAs draw 32x7xlz tiles of all active
-//   solves from one work-queue counter; each solve counts its own tiles, so each keeps its own
-//   lagged dt and clock.  While membership is unchanged the launch sequence of a chunk of steps
+// * A step is two persistent launches per Riemann solver in use (Heun stages; HLLD solves and
+//   HLLC solves in separate launches, so each kernel holds one solver body) whose CTAs draw
+//   32x7xlz tiles of those solves from one work-queue counter; each solve counts its own tiles,
+//   so each keeps its own lagged dt and clock.  While membership is unchanged the launch sequence of a chunk of steps
 //   is replayed from a captured CUDA graph.
 // * The z-march length lz and the persistent grid size are chosen by an autotuner that times
 //   first-stage launches (idempotent: they read U^n and write the stage buffer only).
@@ -106,8 +107,9 @@ struct setb_batch {
     int4* d_items = nullptr;
     int4* h_items = nullptr;       // pinned
     size_t items_cap = 0;
-    int n_items = 0;
-    unsigned* d_queue = nullptr;   // 2 * kMaxGraphSteps counters
+    int n_items = 0;               // work items: HLLD solves' [0, n_hlld), HLLC solves' [n_hlld, n_items)
+    int n_hlld = 0;
+    unsigned* d_queue = nullptr;   // 4 * kMaxGraphSteps counters (2 stages x 2 solvers per step)
     double* d_partial = nullptr;
     double* d_check = nullptr;
     const double** d_rho = nullptr;
@@ -179,7 +181,12 @@ int rebuild(setb_batch* b) {
     for (int s = 0; s < ms; s++)
         if (b->slots[s].active) order.push_back({(long long)b->slots[s].g.nx * b->slots[s].g.ny * b->slots[s].g.nz, s});
     std::sort(order.begin(), order.end(), [](auto& x, auto& y) { return x.first > y.first || (x.first == y.first && x.second < y.second); });
+    // HLLD solves first, then HLLC solves, each largest first: one launch per solver and stage
+    std::stable_partition(order.begin(), order.end(), [&](const std::pair<long long, int>& o) {
+        return b->slots[o.second].opts.n_state == 3;
+    });
     std::vector<int4> items;
+    int n_hlld = 0;
     for (auto& os : order) {
         const int s = os.second;
         Slot& sl = b->slots[s];
@@ -190,6 +197,7 @@ int rebuild(setb_batch* b) {
         for (int bz = 0; bz < ntz; bz++)
             for (int by = 0; by < nty; by++)
                 for (int bx = 0; bx < ntx; bx++) items.push_back(make_int4(s, bx, by, bz));
+        if (sl.opts.n_state == 3) n_hlld = (int)items.size();
         for (int st = 0; st < 2; st++) {
             StageArgs a{};
             a.g = g;
@@ -231,6 +239,7 @@ int rebuild(setb_batch* b) {
     SB_TRY(cudaStreamSynchronize(b->stream));   // pinned staging buffers are about to be rewritten
     if (!items.empty()) std::memcpy(b->h_items, items.data(), sizeof(int4) * items.size());
     b->n_items = (int)items.size();
+    b->n_hlld = n_hlld;
     if (b->n_items) SB_TRY(cudaMemcpyAsync(b->d_items, b->h_items, sizeof(int4) * items.size(), cudaMemcpyHostToDevice, b->stream));
     SB_TRY(cudaMemcpyAsync(b->d_inst1, b->h_inst, sizeof(StageArgs) * ms, cudaMemcpyHostToDevice, b->stream));
     SB_TRY(cudaMemcpyAsync(b->d_inst2, b->h_inst + ms, sizeof(StageArgs) * ms, cudaMemcpyHostToDevice, b->stream));
@@ -239,21 +248,32 @@ int rebuild(setb_batch* b) {
     return SETB_OK;
 }
 
-int grid_size(const setb_batch* b) {
+int grid_size(const setb_batch* b, int n_items) {
     const int g = b->sm_count * batch_ctas_per_sm(b->precision) * b->grid_mult;
-    return std::max(1, std::min(g, std::max(b->n_items, 1)));
+    return std::max(1, std::min(g, std::max(n_items, 1)));
 }
 
-// Enqueues nsteps (<= kMaxGraphSteps) steps: one memset of the queue counters, then 2 launches
-// per step, each with its own counter.
+// Launches one stage over the work items of one solver (n_state 3: HLLD solves, 2: HLLC solves)
+// with queue counter q.
+int launch_items(setb_batch* b, int stage, int n_state, unsigned* q) {
+    const int first = n_state == 3 ? 0 : b->n_hlld;
+    const int n = n_state == 3 ? b->n_hlld : b->n_items - b->n_hlld;
+    if (n == 0) return SETB_OK;
+    BatchArgs a{stage == 1 ? b->d_inst1 : b->d_inst2, b->d_items + first, n, q};
+    SB_TRY(launch_batch_stage(a, b->precision, n_state, stage == 1 ? 0 : 1, stage == 1, grid_size(b, n), b->stream));
+    return SETB_OK;
+}
+
+// Enqueues nsteps (<= kMaxGraphSteps) steps: one memset of the queue counters, then per step and
+// stage one launch per solver that has solves, each with its own counter.
 int enqueue(setb_batch* b, int nsteps) {
-    SB_TRY(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned) * 2 * nsteps, b->stream));
-    const int grid = grid_size(b);
+    SB_TRY(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned) * 4 * nsteps, b->stream));
     for (int s = 0; s < nsteps; s++) {
-        BatchArgs a{b->d_inst1, b->d_items, b->n_items, b->d_queue + 2 * s};
-        SB_TRY(launch_batch_stage(a, b->precision, 0, true, grid, b->stream));
-        BatchArgs c{b->d_inst2, b->d_items, b->n_items, b->d_queue + 2 * s + 1};
-        SB_TRY(launch_batch_stage(c, b->precision, 1, false, grid, b->stream));
+        unsigned* q = b->d_queue + 4 * s;
+        int rc;
+        if ((rc = launch_items(b, 1, 3, q)) || (rc = launch_items(b, 1, 2, q + 1)) ||
+            (rc = launch_items(b, 2, 3, q + 2)) || (rc = launch_items(b, 2, 2, q + 3)))
+            return rc;
     }
     return SETB_OK;
 }
@@ -323,7 +343,7 @@ int32_t setb_batch_create(setb_batch** out, int32_t max_slots, int32_t precision
               cudaMalloc(&b->d_inst1, sizeof(StageArgs) * max_slots) == cudaSuccess &&
               cudaMalloc(&b->d_inst2, sizeof(StageArgs) * max_slots) == cudaSuccess &&
               cudaMallocHost(&b->h_inst, sizeof(StageArgs) * 2 * max_slots) == cudaSuccess &&
-              cudaMalloc(&b->d_queue, sizeof(unsigned) * 2 * kMaxGraphSteps) == cudaSuccess &&
+              cudaMalloc(&b->d_queue, sizeof(unsigned) * 4 * kMaxGraphSteps) == cudaSuccess &&
               cudaMalloc(&b->d_partial, sizeof(double) * 2 * kCheckBlocks * max_slots) == cudaSuccess &&
               cudaMalloc(&b->d_check, sizeof(double) * max_slots) == cudaSuccess &&
               cudaMalloc(&b->d_rho, sizeof(double*) * max_slots) == cudaSuccess &&
@@ -514,7 +534,7 @@ int32_t setb_batch_info(setb_batch* b, int64_t* bytes_used, int32_t* active, int
     if (bytes_used) *bytes_used = b->used;
     if (active) *active = n;
     if (lz) *lz = b->lz;
-    if (grid) *grid = grid_size(b);
+    if (grid) *grid = grid_size(b, b->n_items);
     return SETB_OK;
 }
 
@@ -552,11 +572,9 @@ int32_t setb_batch_tune(setb_batch* b, int32_t reps, int32_t* lz_out, int32_t* g
             b->dirty = true;
             if (rebuild(b)) continue;
             if (b->n_items == 0) continue;
-            const int grid = grid_size(b);
             auto launch_once = [&]() -> bool {
-                if (cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned), b->stream) != cudaSuccess) return false;
-                BatchArgs a{b->d_inst1, b->d_items, b->n_items, b->d_queue};
-                return launch_batch_stage(a, b->precision, 0, true, grid, b->stream) == cudaSuccess;
+                if (cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(unsigned), b->stream) != cudaSuccess) return false;
+                return launch_items(b, 1, 3, b->d_queue) == SETB_OK && launch_items(b, 1, 2, b->d_queue + 1) == SETB_OK;
             };
             if (!launch_once()) continue;   // warm-up
             cudaEventRecord(e0, b->stream);

@@ -385,7 +385,7 @@ cudaError_t launch_stage_fp64(const StageArgs& a, int n_state, int order, int ki
 cudaError_t launch_stage(const StageArgs& a, int precision, int n_state, int order, int kind, bool want_dt,
                          cudaStream_t s);
 int stage_smem_bytes(int precision, int kind);
-cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
+cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int n_state, int kind, bool want_dt, int grid,
                                cudaStream_t s);
 cudaError_t prepare_batch_kernels(int precision);
 int batch_ctas_per_sm(int precision);

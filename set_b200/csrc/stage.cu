@@ -655,9 +655,10 @@ __global__ void __launch_bounds__(Tile<P, KIND>::NT, Tile<P, KIND>::MINB) stage_
 }
 
 // Persistent batch kernel: each CTA takes tiles from the work queue until it is empty; the
-// tile's solve selects the arguments (copied to shared memory) and the Riemann solver.  The
-// items of one solve are counted by its own clock, so every solve keeps its own lagged dt.
-template <int P, int ORDER, int KIND, bool WANT_DT>
+// tile's solve selects the arguments (copied to shared memory).  One launch covers the solves of
+// one Riemann solver (NSTATE), so the kernel holds one solver body.  The items of one solve are
+// counted by its own clock, so every solve keeps its own lagged dt.
+template <int P, int NSTATE, int ORDER, int KIND, bool WANT_DT>
 __global__ void __launch_bounds__(Tile<P, kBatchKind>::NT, Tile<P, kBatchKind>::MINB) batch_stage_kernel(const BatchArgs B) {
     __shared__ __align__(16) StageArgs As;
     __shared__ int4 it;
@@ -679,10 +680,8 @@ __global__ void __launch_bounds__(Tile<P, kBatchKind>::NT, Tile<P, kBatchKind>::
         unsigned long long* dst = reinterpret_cast<unsigned long long*>(&As);
         for (int q = threadIdx.x; q < WORDS; q += Tile<P, kBatchKind>::NT) dst[q] = src[q];
         __syncthreads();
-        if (As.n_state == 3)
-            run_tile<P, 3, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits, tma_dead);
-        else
-            run_tile<P, 2, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits, tma_dead);
+        run_tile<P, NSTATE, ORDER, KIND, WANT_DT, kBatchKind>(As, w.y, w.z, w.w, As.total_tiles, &bar, n_waits,
+                                                              tma_dead);
     }
 }
 
@@ -740,7 +739,10 @@ cudaError_t launch_p(const StageArgs& a, int n_state, int order, int kind, bool 
 
 template <int P, int KIND, bool WANT_DT>
 cudaError_t batch_attr() {
-    return cudaFuncSetAttribute(batch_stage_kernel<P, 2, KIND, WANT_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(batch_stage_kernel<P, 3, 2, KIND, WANT_DT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes<P, kBatchKind>());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(batch_stage_kernel<P, 2, 2, KIND, WANT_DT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem_bytes<P, kBatchKind>());
 }
 
@@ -762,18 +764,24 @@ cudaError_t prepare_batch_kernels(int precision) {
 
 int batch_ctas_per_sm(int precision) { return tile_shape(precision, kBatchKind).ctas_per_sm; }
 
-template <int P>
-void launch_batch_p(const BatchArgs& b, int kind, bool want_dt, int grid, cudaStream_t s) {
+template <int P, int NSTATE>
+void launch_batch_pn(const BatchArgs& b, int kind, bool want_dt, int grid, cudaStream_t s) {
     constexpr int NT = Tile<P, kBatchKind>::NT;
-    if (kind == 0 && want_dt) batch_stage_kernel<P, 2, 0, true><<<grid, NT, smem_bytes<P, kBatchKind>(), s>>>(b);
-    else batch_stage_kernel<P, 2, 1, false><<<grid, NT, smem_bytes<P, kBatchKind>(), s>>>(b);
+    if (kind == 0 && want_dt) batch_stage_kernel<P, NSTATE, 2, 0, true><<<grid, NT, smem_bytes<P, kBatchKind>(), s>>>(b);
+    else batch_stage_kernel<P, NSTATE, 2, 1, false><<<grid, NT, smem_bytes<P, kBatchKind>(), s>>>(b);
 }
 
-cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int kind, bool want_dt, int grid,
+template <int P>
+void launch_batch_p(const BatchArgs& b, int n_state, int kind, bool want_dt, int grid, cudaStream_t s) {
+    if (n_state == 3) launch_batch_pn<P, 3>(b, kind, want_dt, grid, s);
+    else launch_batch_pn<P, 2>(b, kind, want_dt, grid, s);
+}
+
+cudaError_t launch_batch_stage(const BatchArgs& b, int precision, int n_state, int kind, bool want_dt, int grid,
                                cudaStream_t s) {
-    if (precision == 1) launch_batch_p<1>(b, kind, want_dt, grid, s);
-    else if (precision == 2) launch_batch_p<2>(b, kind, want_dt, grid, s);
-    else launch_batch_p<0>(b, kind, want_dt, grid, s);
+    if (precision == 1) launch_batch_p<1>(b, n_state, kind, want_dt, grid, s);
+    else if (precision == 2) launch_batch_p<2>(b, n_state, kind, want_dt, grid, s);
+    else launch_batch_p<0>(b, n_state, kind, want_dt, grid, s);
     return cudaGetLastError();
 }
 
