@@ -37,8 +37,8 @@ struct setb_handle {
     DevStatus* st = nullptr;
     DevClock* h_clk = nullptr;             // pinned mirrors
     DevStatus* h_st = nullptr;
-    CUtensorMap* tmap = nullptr;           // device: [buffer 0/1][tile shape: plain/delta, mixed]
-    bool tma_ok[2] = {false, false};       // per tile shape: maps encoded (else plain loads)
+    CUtensorMap* tmap = nullptr;           // device: [buffer 0/1][tile shape, kShapeTy]
+    bool tma_ok[3] = {false, false, false};   // per tile shape: maps encoded (else plain loads)
     FaceListDev* fl = nullptr;             // face-list grid (g is then 1-D: nx = N cells)
     int ctas_per_sm = 1;
     int sm_count = 148;
@@ -108,9 +108,17 @@ GridGeom make_geom(const setb_cart_desc* d) {
     return g;
 }
 
-// The two tile heights a handle keeps tensor maps for, and which one a launch uses.
-constexpr int kShapeTy[2] = {tile_shape(0, 0).ty, tile_shape(1, 1).ty};
-int shape_index(int precision, int kind) { return tile_shape(precision, kind).ty == kShapeTy[0] ? 0 : 1; }
+// The tile heights a handle keeps tensor maps for (plain, mixed stage 2, mixed stage 1 / delta),
+// and which one a launch uses.
+constexpr int kNumShapes = 3;
+constexpr int kShapeTy[kNumShapes] = {tile_shape(0, 0).ty, tile_shape(1, 1).ty, tile_shape(1, 0).ty};
+constexpr bool shape_listed(int ty) { return ty == kShapeTy[0] || ty == kShapeTy[1] || ty == kShapeTy[2]; }
+static_assert(shape_listed(tile_shape(0, 1).ty) && shape_listed(tile_shape(2, 0).ty) && shape_listed(tile_shape(2, 1).ty),
+              "every stage launch's tile height has a tensor map");
+int shape_index(int precision, int kind) {
+    const int ty = tile_shape(precision, kind).ty;
+    return ty == kShapeTy[0] ? 0 : (ty == kShapeTy[1] ? 1 : 2);
+}
 
 }  // namespace
 
@@ -235,11 +243,11 @@ int create_impl(setb_handle** out, const setb_cart_desc* d, const GridGeom* geo 
         }
     }
     {
-        CUtensorMap tm[4] = {};
-        for (int shape = 0; shape < 2; shape++) {
+        CUtensorMap tm[2 * kNumShapes] = {};
+        for (int shape = 0; shape < kNumShapes; shape++) {
             h->tma_ok[shape] = true;
             for (int b = 0; b < 2; b++)
-                if (encode_state_tmap(h->g, h->buf[b], kShapeTy[shape], &tm[2 * b + shape]) != SETB_OK)
+                if (encode_state_tmap(h->g, h->buf[b], kShapeTy[shape], &tm[kNumShapes * b + shape]) != SETB_OK)
                     h->tma_ok[shape] = false;
         }
         if (cudaMalloc(&h->tmap, sizeof(tm)) != cudaSuccess ||
@@ -629,8 +637,8 @@ int enqueue_steps(setb_handle* h, int32_t nsteps, const setb_step_opts* o, cudaE
     for (int s = 0; s < nsteps; s++) {
         double* U = h->buf[h->cur];
         double* W = h->buf[1 - h->cur];
-        const CUtensorMap* tmU = h->tma_ok[shape0] ? h->tmap + 2 * h->cur + shape0 : nullptr;
-        const CUtensorMap* tmW = h->tma_ok[shape1] ? h->tmap + 2 * (1 - h->cur) + shape1 : nullptr;
+        const CUtensorMap* tmU = h->tma_ok[shape0] ? h->tmap + kNumShapes * h->cur + shape0 : nullptr;
+        const CUtensorMap* tmW = h->tma_ok[shape1] ? h->tmap + kNumShapes * (1 - h->cur) + shape1 : nullptr;
         if (o->scheme == 2) {
             a.g.lz = lz0;
             a.Uin = U;
@@ -902,7 +910,7 @@ int32_t setb_slab_stage(setb_handle* h, int32_t stage, const setb_step_opts* o) 
     a.n_disc = o->n_disc;
     a.copy_wait = h->copy_wait;
     a.Uin = X;
-    a.tm_in = h->tma_ok[shape] ? h->tmap + 2 * in + shape : nullptr;
+    a.tm_in = h->tma_ok[shape] ? h->tmap + kNumShapes * in + shape : nullptr;
     if (stage == 1) {
         a.Ubase = nullptr;
         a.Uout = W;

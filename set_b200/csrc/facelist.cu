@@ -296,7 +296,8 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
                                    dmul(n[2], dadd(q1[7], q2[7])));
             m.divb[gr] = dmul(dmul(0.5, nb), sq);
         }
-        if (WANT_DT) cand = fmin(kDtFaceCap, cfl * dist * sb_rcp(fmax(fabs(sp[0]), fabs(sp[1]))));
+        // compare-and-select min / max (the library fmin / fmax of doubles are far longer sequences)
+        if (WANT_DT) cand = sb_min(kDtFaceCap, cfl * dist * sb_rcp(sb_max(fabs(sp[0]), fabs(sp[1]))));
     }
     if (n_recon) atomicAdd(&cnt[0], (unsigned long long)n_recon);
     if (n_wave) atomicAdd(&cnt[1], (unsigned long long)n_wave);
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(kCellThreads) fl_cell_kernel(const FaceListDev
                 prim_from_cons(un, q, ke, me);
                 if (q[4] <= 0.0) {
                     atomicAdd(&cnt[1], 1ull);
-                    un[4] = (kPFloor * kInvG1 + ke) + me;
+                    un[4] = floor_energy(ke, me);
                 }
             }
         }

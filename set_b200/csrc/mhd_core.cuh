@@ -161,14 +161,24 @@ template <typename T> SB_HD T sb_max(T a, T b) { return a < b ? b : a; }
 template <typename T> SB_HD T sb_pos(T x) { return x > T(0) ? x : T(0); }
 
 // Solvers.f90:126-137: (signum(x)+signum(y))/2 * min(|x|,|y|).  On the device it is branch-free
-// in both precisions: |minmod| = max(0, min(|a|, b * sign(a))) with the sign of a (the same value
-// for every finite a, b, except that a zero result may carry a's sign).  In the FP64 stage kernel
-// the compare-and-branch form cost 16 % of the plain form's time (A/B on one box: 2.41 -> 2.81 G
-// cell-updates/s at 256^3), through divergent branches in the 30 minmods per cell and stage.
+// (the same value for every finite a, b, except that a zero result may carry a sign); in the FP64
+// stage kernel the compare-and-branch form cost 16 % of the plain form's time (A/B on one box:
+// 2.41 -> 2.81 G cell-updates/s at 256^3), through divergent branches in the 30 minmods per cell
+// and stage.  FP32: |minmod| = max(0, min(|a|, b * sign(a))) with the sign of a.  FP64 works on
+// the bit patterns, on the integer pipes: the FP64 pipe is the plain form's bottleneck, and
+// minmod's value is one of its arguments (or zero), so no FP64 operation is needed -- with the
+// signs of a and b different the result is 0, else the argument of smaller magnitude (magnitudes
+// of doubles order like their bit patterns with the sign bit cleared).
 template <typename T> SB_HD T minmod(T a, T b) {
 #if defined(__CUDA_ARCH__)
-    if constexpr (sizeof(T) == 4) return copysignf(fmaxf(0.0f, fminf(fabsf(a), b * copysignf(1.0f, a))), a);
-    else return copysign(fmax(0.0, fmin(fabs(a), b * copysign(1.0, a))), a);
+    if constexpr (sizeof(T) == 4) {
+        return copysignf(fmaxf(0.0f, fminf(fabsf(a), b * copysignf(1.0f, a))), a);
+    } else {
+        const long long A = __double_as_longlong(a), B = __double_as_longlong(b);
+        const unsigned long long kMag = 0x7fffffffffffffffull;
+        const long long m = ((unsigned long long)A & kMag) < ((unsigned long long)B & kMag) ? A : B;
+        return (A ^ B) < 0 ? 0.0 : __longlong_as_double(m);
+    }
 #endif
     if (a > T(0) && b > T(0)) return sb_min(a, b);
     if (a < T(0) && b < T(0)) return sb_max(a, b);
@@ -176,25 +186,96 @@ template <typename T> SB_HD T minmod(T a, T b) {
 }
 
 // ------------------------------------------------------------------ conserved -> primitive
+// Explicitly rounded FP64 operations (no FMA contraction), for arithmetic that must match a
+// host evaluation bit for bit.
+SB_HD double rn_mul(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+SB_HD double rn_add(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+SB_HD double rn_sub(double a, double b) {
+#if defined(__CUDA_ARCH__)
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+// a / b rounded to nearest, given y = RN(1/b): q = RN(a y), the remainder r = a - b q is exact
+// under FMA, and RN(q + r y) = RN(a / b) (Markstein's quotient theorem: y within half an ulp of
+// 1/b and q within one ulp of a/b; IBM J. Res. Dev. 34(1), 1990).  Three operations per quotient
+// after one shared reciprocal; tests/test_gpu_special.py compares it with IEEE division.
+SB_HD double div_rn(double a, double b, double y) {
+#if defined(__CUDA_ARCH__)
+    const double q = __dmul_rn(a, y);
+    // the sign of q is the quotient's (a zero numerator keeps its sign, which the correction
+    // step's zero sum would drop)
+    return copysign(__fma_rn(__fma_rn(-q, b, a), y, q), q);
+#else
+    (void)y;
+    return a / b;
+#endif
+}
+
 // U = (rho, mx, my, mz, E, Bx, By, Bz), B in stored units, E carrying |B/sqrt(4pi)|^2/2.
 // Pressure recovery: p = ((E - rho|v|^2/2) - |b|^2/2)(gamma-1)  (cuf_solvers.cuf:735-738 with the
 // magnetic term of the conservative MHD energy).
+// EXACT (the plain form's default): the velocities and b are the correctly rounded quotients
+// U[1..3] / rho and B / sqrt(4 pi), and ke, me, p are evaluated in the written order with every
+// operation rounded, so the primitive state equals the host evaluation (the oracle's) bit for
+// bit.  Pressure recovery cancels where the flow is hypersonic (the solar-wind source's outflow
+// runs at Mach ~77, where rho|v|^2/2 is ~3000 times p): there one ulp in a velocity moves p by
+// ~1e-12 relative, so a step computed from a differently rounded p differs from another correct
+// FP64 step by more than 1e-12 per cell.  !EXACT: one reciprocal and multiplies, with
+// contraction (the mixed form, which rounds the result to FP32).
+// SB: q[5..7] = b = B / sqrt(4 pi) (the field in the units the Riemann solver works in) instead of
+// the stored B.
+template <bool EXACT = true, bool SB = false>
 SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
     const double rho = U[0];
     const double ir = sb_rcp(rho);
-    const double u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
-    const double bx = U[5] * kInvSpi4, by = U[6] * kInvSpi4, bz = U[7] * kInvSpi4;
-    ke = 0.5 * rho * ((u * u + v * v) + w * w);
-    me = 0.5 * ((bx * bx + by * by) + bz * bz);
+    double u, v, w, bx, by, bz;
+    if (EXACT) {
+        u = div_rn(U[1], rho, ir);
+        v = div_rn(U[2], rho, ir);
+        w = div_rn(U[3], rho, ir);
+        bx = div_rn(U[5], kSpi4, kInvSpi4);
+        by = div_rn(U[6], kSpi4, kInvSpi4);
+        bz = div_rn(U[7], kSpi4, kInvSpi4);
+        ke = rn_mul(rn_mul(0.5, rho), rn_add(rn_add(rn_mul(u, u), rn_mul(v, v)), rn_mul(w, w)));
+        me = rn_mul(0.5, rn_add(rn_add(rn_mul(bx, bx), rn_mul(by, by)), rn_mul(bz, bz)));
+        q[4] = rn_mul(rn_sub(rn_sub(U[4], ke), me), kG1);
+    } else {
+        u = U[1] * ir;
+        v = U[2] * ir;
+        w = U[3] * ir;
+        bx = U[5] * kInvSpi4;
+        by = U[6] * kInvSpi4;
+        bz = U[7] * kInvSpi4;
+        ke = 0.5 * rho * ((u * u + v * v) + w * w);
+        me = 0.5 * ((bx * bx + by * by) + bz * bz);
+        q[4] = ((U[4] - ke) - me) * kG1;
+    }
     q[0] = rho;
     q[1] = u;
     q[2] = v;
     q[3] = w;
-    q[4] = ((U[4] - ke) - me) * kG1;
-    q[5] = U[5];
-    q[6] = U[6];
-    q[7] = U[7];
+    q[5] = SB ? bx : U[5];
+    q[6] = SB ? by : U[6];
+    q[7] = SB ? bz : U[7];
 }
+// Total energy at the pressure floor, (p_floor/(gamma-1) + ke) + me: the oracle's cons_from_prim
+// of the floored state (cuf_solvers.cuf:777-779), with ke, me from prim_from_cons<true>.
+constexpr double kPFloorE = kPFloor / kG1;
+SB_HD double floor_energy(double ke, double me) { return rn_add(rn_add(kPFloorE, ke), me); }
 
 // ------------------------------------------------------------------ Riemann solver
 // Face-frame states q = (rho, vn, vt1, vt2, p, Bn, Bt1, Bt2), B in stored units.
@@ -202,7 +283,8 @@ SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
 // SL, SR, SM (chlld's dsl, dsp, dsc).  wv is the face speed (used only when MOVING).
 // Returns a bit set: kFlagWave when no wave-fan region matched (the reference STOPs),
 // kFlagStar (CHECK_STAR only) when the selected state has rho <= 0 or p <= 0 or F is not finite.
-template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR, bool NR = true>
+// BS: the states carry b = B / sqrt(4 pi) already (q[5..7]), so the solver skips its scaling.
+template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR, bool NR = true, bool BS = false>
 SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& SRo, T& SMo) {
     const T ispi4 = T(kInvSpi4);
     const T ga = T(kGamma);
@@ -212,9 +294,9 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     if (!MOVING) wv = T(0);
 
     const T r1 = q1[0], u1 = q1[1], v1 = q1[2], w1 = q1[3], p1 = q1[4];
-    const T bx1 = q1[5] * ispi4, by1 = q1[6] * ispi4, bz1 = q1[7] * ispi4;
+    const T bx1 = BS ? q1[5] : q1[5] * ispi4, by1 = BS ? q1[6] : q1[6] * ispi4, bz1 = BS ? q1[7] : q1[7] * ispi4;
     const T r2 = q2[0], u2 = q2[1], v2 = q2[2], w2 = q2[3], p2 = q2[4];
-    const T bx2 = q2[5] * ispi4, by2 = q2[6] * ispi4, bz2 = q2[7] * ispi4;
+    const T bx2 = BS ? q2[5] : q2[5] * ispi4, by2 = BS ? q2[6] : q2[6] * ispi4, bz2 = BS ? q2[7] : q2[7] * ispi4;
 
     // fast magnetosonic speeds, Solvers.f90:1282-1306.  The reference forms
     // cf = (sqrt(b2/r + c(c + 2a)) + sqrt(b2/r + c(c - 2a)))/2 with c = sqrt(ga p/r),

@@ -158,8 +158,11 @@ extern "C" int32_t setb_step_noalloc(const setb_cart_desc* d, const setb_step_op
         }
         if (e != cudaSuccess) return SETB_ECUDA;
     }
-    if (cur != U &&
-        cudaMemcpyAsync(U, cur, sizeof(double) * 8 * (size_t)var_stride, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    // an odd number of Euler steps ends in the scratch: copy the N cells of each plane back (the
+    // scratch's plane padding holds whatever an earlier call left there; the caller's padding is
+    // never written)
+    if (cur != U && cudaMemcpy2DAsync(U, sizeof(double) * (size_t)var_stride, cur, sizeof(double) * (size_t)var_stride,
+                                      sizeof(double) * (size_t)N, 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
         return SETB_ECUDA;
     unsigned char hdr[sizeof(DevClock) + sizeof(DevStatus)];
     if (cudaMemcpyAsync(hdr, scratch, sizeof(hdr), cudaMemcpyDeviceToHost, s) != cudaSuccess ||

@@ -15,7 +15,8 @@
 //   * the conservative update, p floor, source re-imposition and the dt candidate reduction
 //     (warp shuffle -> one atomicMin per CTA) are fused; the last CTA rolls the lagged-dt clock.
 //
-// P = 0, plain form: everything in FP64.
+// P = 0, plain form: everything in FP64; the ring holds the field as b = B / sqrt(4 pi), the units
+//   the Riemann solver works in, and the primitives are recovered exactly as the oracle does.
 // P = 1, mixed form: the ring holds FP32 primitives (recovered from the FP64 state in FP64),
 //   reconstruction and the Riemann solver run in FP32, fluxes are stored in FP32; a face whose
 //   selected FP32 state has rho <= 0 or p <= 0 (or a non-finite flux) is recomputed in FP64 from
@@ -50,13 +51,21 @@ constexpr int RING = 4;
 
 __device__ __forceinline__ int ring_slot(int k) { return (k + 4 * RING) & (RING - 1); }
 
+// The inflow ghost state beyond x = hi as a primitive ring entry: stored B, or with SB the
+// solver's b = B / sqrt(4 pi) (correctly rounded, as prim_from_cons<true, true> forms it).
+template <bool SB>
+__device__ __forceinline__ void inflow_prim(const GridGeom& g, double* q) {
+#pragma unroll
+    for (int v = 0; v < 8; v++) q[v] = (SB && v >= 5) ? div_rn(g.inflow[v], kSpi4, kInvSpi4) : g.inflow[v];
+}
+
 // FP64 primitive state of global cell (i,j,k) with the boundary rules: inflow beyond x = hi,
-// zero-gradient (clamped index) elsewhere.
+// zero-gradient (clamped index) elsewhere.  SB: the field as b (see prim_from_cons).
+template <bool EXACT, bool SB = false>
 __device__ __forceinline__ void fetch_prim64(const StageArgs& A, int i, int j, int k, double* q) {
     const GridGeom& g = A.g;
     if (i >= g.nx) {
-#pragma unroll
-        for (int v = 0; v < 8; v++) q[v] = g.inflow[v];
+        inflow_prim<SB>(g, q);
         return;
     }
     i = max(i, 0);
@@ -67,7 +76,7 @@ __device__ __forceinline__ void fetch_prim64(const StageArgs& A, int i, int j, i
 #pragma unroll
     for (int v = 0; v < 8; v++) U[v] = __ldg(A.Uin + v * g.vs + off);
     double ke, me;
-    prim_from_cons(U, q, ke, me);
+    prim_from_cons<EXACT, SB>(U, q, ke, me);
 }
 
 // Loads plane kk (with halo) of the tile starting at (i0, j0) as primitives into `dst`.
@@ -77,7 +86,7 @@ __device__ __forceinline__ void load_plane(const StageArgs& A, RT* dst, int i0, 
     for (int c = threadIdx.x; c < PLANE; c += NT) {
         const int cx = c % HX, cy = c / HX;
         double q[8];
-        fetch_prim64(A, i0 - 2 + cx, j0 - 2 + cy, kk, q);
+        fetch_prim64<P != 1, P == 0>(A, i0 - 2 + cx, j0 - 2 + cy, kk, q);
 #pragma unroll
         for (int v = 0; v < 8; v++) dst[v * PLANE + c] = (RT)q[v];
     }
@@ -152,8 +161,7 @@ __device__ __forceinline__ void convert_plane(const StageArgs& A, const double* 
         const int i = i0 - 2 + cx, j = j0 - 2 + cy;
         double q[8];
         if (i >= g.nx) {
-#pragma unroll
-            for (int v = 0; v < 8; v++) q[v] = g.inflow[v];
+            inflow_prim<P == 0>(g, q);
         } else {
             const int sx = max(i, 0) - (i0 - 2), sy = min(max(j, 0), g.ny - 1) - (j0 - 2);
             const double* src = stg + sy * HX + sx;
@@ -161,7 +169,7 @@ __device__ __forceinline__ void convert_plane(const StageArgs& A, const double* 
 #pragma unroll
             for (int v = 0; v < 8; v++) U[v] = src[v * PLANE];
             double ke, me;
-            prim_from_cons(U, q, ke, me);
+            prim_from_cons<P != 1, P == 0>(U, q, ke, me);
         }
 #pragma unroll
         for (int v = 0; v < 8; v++) dst[v * PLANE + c] = (RT)q[v];
@@ -309,8 +317,11 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     constexpr int TX = C::TX, TY = C::TY, NC = C::NC, NT = C::NT, HX = C::HX, PLANE = C::PLANE;
     constexpr int NXF = C::NXF, NYF = C::NYF;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // [8][PLANE] staged conserved box; tensor copies land on a 128-byte aligned address
-    double* stg = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    // [8][PLANE] staged conserved box; tensor copies land on a 128-byte aligned address.  The
+    // alignment pad is an offset from the shared array itself, so every pointer below stays in
+    // the shared address space (shared loads and stores with 32-bit addresses, not generic ones).
+    const unsigned pad = (128u - (smem_u32(smem_raw) & 127u)) & 127u;
+    double* stg = reinterpret_cast<double*>(smem_raw + pad);
     RG* ring = reinterpret_cast<RG*>(stg + 8 * PLANE);
     FT* fx = reinterpret_cast<FT*>(ring + RING * 8 * PLANE);   // [8][NXF]
     FT* fy = fx + 8 * NXF;                                      // [8][NYF]
@@ -427,7 +438,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                 else
                     fl = riemann<RT, NSTATE, false, true>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
             } else {
-                fl = riemann<RT, NSTATE, false, P == 1>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+                // the plain form's ring holds b = B / sqrt(4 pi) (BS)
+                fl = riemann<RT, NSTATE, false, P == 1, true, P == 0>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
             }
             sl = (double)SL;
             sr = (double)SR;
@@ -451,7 +463,9 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             else scatter_face<1, NYF>(out + oidx, F, (RT)sq);
         }
         if ((fl & kFlagWave) && real && !dup) n_wave++;
-        if (WANT_DT && real) rate = fmax(rate, fmax(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
+        // compare-and-select maxima (the library fmax of doubles is a far longer sequence); a NaN
+        // speed is skipped, as fmax would skip it
+        if (WANT_DT && real) rate = sb_max(rate, sb_max(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
     };
 
     // ---- the march over planes kk = k0-2 .. k1+1.  Plane kk enters ring slot kk; from
@@ -574,10 +588,10 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                     reset_comp = true;
                 } else {
                     double q[8], ke, me;
-                    prim_from_cons(un, q, ke, me);
+                    prim_from_cons<P != 1>(un, q, ke, me);
                     if (q[4] <= 0.0) {                    // cuf_solvers.cuf:777-779
                         atomicAdd(&cnt[1], 1ull);
-                        un[4] = (kPFloor * kInvG1 + ke) + me;
+                        un[4] = floor_energy(ke, me);
                         cmp[4] = 0.0;
                     }
                 }

@@ -1,5 +1,7 @@
 """The plain form's FP64 special functions on the device (set_b200/csrc/mhd_core.cuh: rs_rcp,
-rs_rsqrt, rs_sqrt: Newton-refined approximate instructions) against IEEE results.
+rs_rsqrt, rs_sqrt: Newton-refined approximate instructions) against IEEE results; its quotient
+from a shared correctly rounded reciprocal (div_rn) against IEEE division; and its exact primitive
+recovery (prim_from_cons<true>) against the oracle's, bit for bit.
 
 tests/csrc/rs_special.cu wraps them in a kernel; this test compiles it with nvcc for sm_100a
 into a temporary library.  The reference values are numpy's correctly rounded 1/x and sqrt(x),
@@ -28,8 +30,13 @@ def rs_lib(tmp_path_factory):
                            "-Xcompiler", "-fPIC", "-shared", "-I" + CSRC,
                            os.path.join(HERE, "csrc", "rs_special.cu"), "-o", out])
     lib = C.CDLL(out)
+    dp = C.POINTER(C.c_double)
     lib.rs_eval.restype = C.c_int
-    lib.rs_eval.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_longlong]
+    lib.rs_eval.argtypes = [dp, dp, C.c_longlong]
+    lib.div_eval.restype = C.c_int
+    lib.div_eval.argtypes = [dp, dp, dp, C.c_longlong]
+    lib.prim_eval.restype = C.c_int
+    lib.prim_eval.argtypes = [dp, dp, C.c_longlong]
     return lib
 
 
@@ -73,3 +80,49 @@ def test_special_functions_outside_their_domain(rs_lib):
     r = rs_eval(rs_lib, edge)
     assert r[0, 2] == 0.0
     assert np.isnan(r[:, 0]).all() and np.isnan(r[:, 1]).all()
+
+
+def _p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def test_quotient_from_shared_reciprocal_is_ieee_division(rs_lib):
+    """div_rn(a, b, RN(1/b)) equals the device's IEEE a / b bit for bit: quotients over 1e-150..1e150
+    of both signs, and the state's own range (velocities of momenta over densities)."""
+    rng = np.random.default_rng(2)
+    n = 1 << 20
+    a = np.concatenate([rng.choice([-1.0, 1.0], n) * 10.0 ** rng.uniform(-150, 150, n),
+                        rng.normal(0.0, 500.0, n)])
+    b = np.concatenate([rng.choice([-1.0, 1.0], n) * 10.0 ** rng.uniform(-150, 150, n),
+                        10.0 ** rng.uniform(-4, 4, n)])
+    a[:7] = [0.0, -0.0, 1.0, 3.0, 7.0, 1.0, 0.1]
+    b[:7] = [3.0, 5.0, 3.0, 3.0, 3.0, 1.0 - 2.0 ** -53, 3.5449077018110318]
+    out = np.zeros(2 * a.size)
+    assert rs_lib.div_eval(_p(a), _p(b), _p(out), a.size) == 0
+    got, ieee = out[0::2], out[1::2]
+    np.testing.assert_array_equal(got.view(np.int64), ieee.view(np.int64))
+    np.testing.assert_array_equal(ieee, a / b)   # the device's division is numpy's
+
+
+def test_exact_primitive_recovery_matches_the_oracle(rs_lib):
+    """prim_from_cons<true> on the device equals the oracle's prim_from_cons bit for bit,
+    including hypersonic states whose pressure is ~1e-4 of the kinetic energy (where one ulp of
+    a velocity moves p by ~1e-12)."""
+    import oracle as O
+    rng = np.random.default_rng(3)
+    n = 1 << 16
+    rho = 10.0 ** rng.uniform(-3, 2, n)
+    v = rng.normal(0.0, 3.0, (n, 3)) * np.where(rng.uniform(size=n) < 0.3, 5.0, 1.0)[:, None]
+    B = rng.normal(0.0, 1.0, (n, 3)) * (rng.uniform(size=n) < 0.7)[:, None]
+    ke = 0.5 * rho * (v ** 2).sum(1)
+    me = 0.5 * (B ** 2).sum(1) / (4 * np.pi)
+    p = (ke + me) * 10.0 ** rng.uniform(-4, 1, n)
+    U = np.zeros((n, 8))
+    U[:, 0] = rho
+    U[:, 1:4] = rho[:, None] * v
+    U[:, 4] = p / (2.0 / 3.0) + ke + me
+    U[:, 5:8] = B
+    got = np.zeros((n, 8))
+    assert rs_lib.prim_eval(_p(U), _p(got), n) == 0
+    ref = np.array([O.prim_from_cons(U[i]) for i in range(n)])
+    np.testing.assert_array_equal(got.view(np.int64), ref.view(np.int64))
