@@ -90,27 +90,27 @@ SB_HD float sb_rsqrt(float x) {
 #endif
 }
 // The Riemann solver's special functions.  FP32: the approximations above.  FP64 on the device:
-// the FP64 approximate instructions (relative error ~1e-6, measured) refined by Newton-Raphson
-// iteration -- two steps y <- y + y (1 - x y) for 1/x, two steps y <- y + (y/2)(1 - x y^2) for
-// 1/sqrt(x) -- and sqrt(x) as x y after one such step, corrected by one step of Heron's method
-// s <- s + (y/2)(x - s^2).  Domain: positive normal x whose result is normal (the approximate
-// instructions flush subnormals); there 1/x and sqrt(x) are correctly rounded and 1/sqrt(x) is
-// within 1 ulp (tests/test_gpu_special.py checks 2^20 inputs over 1e-300..1e300).  At 0, +-inf
-// and subnormals 1/x and 1/sqrt(x) give NaN (sqrt(0) = 0).  Every argument the flux passes them
-// is a positive density, a sum of squares under sb_pos, or a wave-speed difference that a valid
-// state keeps away from zero (SR - SL >= cfL + cfR > 0; the star denominators tt are screened
-// against 1e-9 before the reciprocal); a state that is already invalid (rho <= 0) is reported by
-// the cell update's counters either way.  These dependent fused
-// multiply-adds are a shorter chain than the correctly rounded library forms, which the FP64
-// flux's latency-bound schedule rewards; the state conversions and the mixed form keep the
-// library forms (there the Newton forms measured slower).  On the host all three are the IEEE
-// operations.
+// the FP64 approximate instructions (relative error ~1e-6, measured) refined by one third-order
+// step each -- 1/x = y (1 + e + e^2) with e = 1 - x y, and 1/sqrt(x) = y (1 + e/2 + 3e^2/8) with
+// e = 1 - x y^2 (the truncated binomial series: ~e^3 ~ 2^-60 before the final rounding; e is
+// formed with one rounding of x y, ~2^-54 relative) -- and sqrt(x) = x * (1/sqrt(x)).  Domain:
+// positive normal x whose result is normal (the approximate instructions flush subnormals);
+// there 1/x and 1/sqrt(x) are within one ulp and sqrt(x) within two, mostly correctly rounded
+// (tests/test_gpu_special.py checks 2^20 inputs over 1e-300..1e300).  At 0 and +-inf 1/x and
+// 1/sqrt(x) give NaN; at subnormals 1/x gives NaN and 1/sqrt(x) +inf (sqrt(0) = 0).  Every argument the flux passes them is a positive density, a sum of squares
+// under sb_pos, or a wave-speed difference that a valid state keeps away from zero (SR - SL >=
+// cfL + cfR > 0; the star denominators tt are screened against 1e-9 before the reciprocal); a
+// state that is already invalid (rho <= 0) is reported by the cell update's counters either way.
+// Three (1/x), five (1/sqrt(x)) and six (sqrt(x)) FP64 operations after the seed: fewer than the
+// correctly rounded library forms, on the pipe that bounds the plain form; the state conversions,
+// the mixed form and the out-of-line FP64 recomputes keep the library forms.  On the host all
+// three are the IEEE operations.
 SB_HD double rs_rcp(double x) {
 #if defined(__CUDA_ARCH__)
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    y = fma(y, fma(-x, y, 1.0), y);
-    return fma(y, fma(-x, y, 1.0), y);
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
 #else
     return 1.0 / x;
 #endif
@@ -119,19 +119,15 @@ SB_HD double rs_rsqrt(double x) {
 #if defined(__CUDA_ARCH__)
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
-    return fma(0.5 * y, fma(-x * y, y, 1.0), y);
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y, e * fma(0.375, e, 0.5), y);
 #else
     return 1.0 / std::sqrt(x);
 #endif
 }
 SB_HD double rs_sqrt(double x) {
 #if defined(__CUDA_ARCH__)
-    double y;
-    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    y = fma(0.5 * y, fma(-x * y, y, 1.0), y);
-    const double s = x * y;
-    const double r = fma(0.5 * y, fma(-s, s, x), s);
+    const double r = x * rs_rsqrt(x);
     return x == 0.0 ? x : r;   // the seed of 0 is infinite
 #else
     return std::sqrt(x);
@@ -155,10 +151,32 @@ template <bool NR, typename T> SB_HD T fr_sqrt(T x) {
     else return sb_sqrt(x);
 }
 
-template <typename T> SB_HD T sb_abs(T x) { return x < T(0) ? -x : x; }
+// |x| is a sign-bit operation on the device; sb_pos of a double tests the sign on the integer
+// pipes (the FP64 pipe is the plain form's bottleneck): the same value for every non-NaN x.
+template <typename T> SB_HD T sb_abs(T x) {
+#if defined(__CUDA_ARCH__)
+    return fabs(x);
+#else
+    return x < T(0) ? -x : x;
+#endif
+}
 template <typename T> SB_HD T sb_min(T a, T b) { return b < a ? b : a; }
 template <typename T> SB_HD T sb_max(T a, T b) { return a < b ? b : a; }
-template <typename T> SB_HD T sb_pos(T x) { return x > T(0) ? x : T(0); }
+template <typename T> SB_HD T sb_pos(T x) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 8) return __double_as_longlong(x) > 0 ? x : T(0);
+#endif
+    return x > T(0) ? x : T(0);
+}
+// x < 0; a double on the device is tested by its sign bit (integer pipes), which differs from
+// the comparison only at -0 and at NaNs with the sign bit set -- values no valid density or
+// pressure takes.
+template <typename T> SB_HD bool sb_neg(T x) {
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 8) return __double_as_longlong(x) < 0;
+#endif
+    return x < T(0);
+}
 
 // Solvers.f90:126-137: (signum(x)+signum(y))/2 * min(|x|,|y|).  On the device it is branch-free
 // (the same value for every finite a, b, except that a zero result may carry a sign); in the FP64
@@ -815,10 +833,10 @@ SB_HD void reconstruct(const T* qLL, const T* qL, const T* qR, const T* qRR, T* 
             q1[v] = muscl(qLL[v], qL[v], qR[v]);
             q2[v] = muscl(qRR[v], qR[v], qL[v]);
         }
-        if (q1[0] < T(0)) q1[0] = qL[0];
-        if (q1[4] < T(0)) q1[4] = qL[4];
-        if (q2[0] < T(0)) q2[0] = qR[0];
-        if (q2[4] < T(0)) q2[4] = qR[4];
+        if (sb_neg(q1[0])) q1[0] = qL[0];
+        if (sb_neg(q1[4])) q1[4] = qL[4];
+        if (sb_neg(q2[0])) q2[0] = qR[0];
+        if (sb_neg(q2[4])) q2[4] = qR[4];
     }
 }
 
