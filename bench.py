@@ -42,9 +42,12 @@ BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
 BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
 BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
 # DRAM bytes (read + write) per cell of one plain stage-2 launch, from an ncu capture of that
-# kernel at 160^3 (774.07 MB / 4.096 M cells); traffic grows with the cell count, so the
-# full-size launch's traffic is this figure times its cells.
-TRAFFIC_STAGE2_PER_CELL = 774.065152e6 / 160 ** 3
+# kernel at 160^3 (1.0407 TB/s x 743.4 us = 773.6 MB / 4.096 M cells); traffic grows with the
+# cell count, so the full-size launch's traffic is this figure times its cells.
+TRAFFIC_STAGE2_PER_CELL = 773.6e6 / 160 ** 3
+# FP64 pipe thread instructions (DFMA + DMUL + DADD + DSETP) per cell of the same launch, from
+# the same capture's opcode counts (163.73 M warp instructions x 30.88 threads / 4.096 M cells).
+FP64_OPS_STAGE2_PER_CELL = 1234
 
 
 def peaks():
@@ -421,6 +424,12 @@ def run_ours(args, world, rank, local):
     t2 = k_ms[1] / max(k_n[1], 1)
     ach2 = BYTES_STAGE2 * cells / (t2 / 1e3) / 1e9
     ach_step = BYTES_STEP * cells / ((t1 + t2) / 1e3) / 1e9
+    # the pipe that bounds the kernel: FP64 operations of the stage-2 launch (counted by ncu)
+    # against 64 FP64 lanes per SM per clock at the sampled SM clock
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    sm_hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    fp64_ach = FP64_OPS_STAGE2_PER_CELL * cells / (t2 / 1e3) / 1e12
+    fp64_peak = 64 * sms * sm_hz / 1e12
 
     # ---- mixed form on the same workload: speed and L1 density error against the plain run
     mixed = None
@@ -554,8 +563,12 @@ def run_ours(args, world, rank, local):
                                            "scaled by cells",
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
                          "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
-                         "limiter": "FP64 latency and issue, not DRAM: at 160^3 ncu shows DRAM traffic 0.98x "
-                                    "algorithmic, FP64 pipe 40-42 %, issue 50-53 % at 12 warps/SM"},
+                         "limiter": "the FP64 pipe and instruction issue, not DRAM: at 160^3 ncu shows DRAM "
+                                    "traffic 0.98x algorithmic, FP64 pipe 42-44 %, issue 47-48 % at 12 warps/SM",
+                         "fp64_pipe": {"ops_per_cell": FP64_OPS_STAGE2_PER_CELL, "achieved_tops": fp64_ach,
+                                       "peak_tops": fp64_peak, "frac": fp64_ach / fp64_peak,
+                                       "source": "DFMA + DMUL + DADD + DSETP thread instructions per cell of the "
+                                                 "stage-2 launch (ncu at 160^3); peak 64 lanes per SM clock"}},
             "mixed": mixed,
             "c3": c3,
             "ensemble": ensemble,
