@@ -263,12 +263,15 @@ def run_c5(args):
     keep = [k for k, r in enumerate(reqs) if r.inst.desc.nx <= 160]
     out = SV.run_stream(reqs, max_slots=256, precision=1, keep=keep)
     t0 = time.perf_counter()
-    l1, same_steps, seq_steps, seq_conv = [], 0, [], 0
+    l1, same_steps, seq_steps, seq_conv, seq_failed, both_failed = [], 0, [], 0, 0, 0
     for k, rq in enumerate(reqs):
         alone = SV.solve_alone(rq.inst, 0, rq.steady_tol, rq.max_steps, keep_state=k in out["states"])
         seq_steps.append(alone["steps"])
         seq_conv += int(alone["converged"])
-        if k in out["states"] and alone["steps"] == out["steps"][k] and out["results"][k].status == 0:
+        seq_failed += int(alone["status"] != 0)
+        both_failed += int(alone["status"] != 0 and out["results"][k].status != 0)
+        if (k in out["states"] and alone["steps"] == out["steps"][k] and out["results"][k].status == 0
+                and alone["status"] == 0):
             a, b = alone["U"][0], out["states"][k][0]
             l1.append(float(np.abs(b - a).sum() / np.abs(a).sum()))
             same_steps += 1
@@ -283,7 +286,8 @@ def run_c5(args):
             "converged": out["converged"], "failed": out["failed"], "failed_by_status": out["failed_by_status"],
             "steps_mean": float(np.mean(out["steps"])),
             "sequential_plain_solves_per_s": len(reqs) / seq_secs, "sequential_plain_seconds": seq_secs,
-            "sequential_plain_converged": seq_conv,
+            "sequential_plain_converged": seq_conv, "sequential_plain_failed": seq_failed,
+            "failed_in_both": both_failed,
             "speedup_vs_sequential_plain": out["solves_per_s"] / (len(reqs) / seq_secs),
             "l1_rho_served_vs_plain": {"compared": same_steps, "max": max(l1) if l1 else None,
                                        "median": float(np.median(l1)) if l1 else None}}

@@ -267,21 +267,22 @@ __global__ void __launch_bounds__(kFaceThreads, 4) fl_face_kernel(const FaceList
                 t1[v] = linear_rcp(ra1, q11[v], -df1, q1[v], rb, q2[v]);
                 t2[v] = linear_rcp(ra2, q22[v], -df2, q2[v], rb, q1[v]);
             }
-            if (t1[0] < 0.0) t1[0] = q1[0];
-            if (t1[4] < 0.0) t1[4] = q1[4];
-            if (t2[0] < 0.0) t2[0] = q2[0];
-            if (t2[4] < 0.0) t2[4] = q2[4];
+            if (sb_neg(t1[0])) t1[0] = q1[0];
+            if (sb_neg(t1[4])) t1[4] = q1[4];
+            if (sb_neg(t2[0])) t2[0] = q2[0];
+            if (sb_neg(t2[4])) t2[4] = q2[4];
 #pragma unroll
             for (int v = 0; v < 5; v++) {
                 q1[v] = t1[v];
                 q2[v] = t2[v];
             }
         }
-        if (q1[0] < 0.0 || q2[0] < 0.0) n_recon++;
+        if (sb_neg(q1[0]) || sb_neg(q2[0])) n_recon++;
         double qqq[8], sp[3];
         int32_t fl = 0;
-        if (tword & kLaxFace) chlld_general<double, 0>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);   // :293-295
-        else chlld_general<double, NSTATE>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);
+        // the faces do not move (w = 0): no face-speed terms
+        if (tword & kLaxFace) chlld_general<double, 0, false, false>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);   // :293-295
+        else chlld_general<double, NSTATE, false, false>(n, 0.0, q1, q2, n_disc, qqq, sp, &fl);
         if (fl & kFlagWave) {
             n_wave++;
 #pragma unroll

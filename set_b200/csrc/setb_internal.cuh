@@ -290,8 +290,9 @@ SB_HD void face_basis(const double* nrm, const double* q1d, const double* q2d, d
 }
 
 // General-normal chlld for a batch of faces: the lab states are rotated into an orthonormal
-// face frame (face_basis), solved, and the momentum / B fluxes rotated back.
-template <typename T, int NSTATE, bool DELTA = false>
+// face frame (face_basis), solved, and the momentum / B fluxes rotated back.  MOVING = false:
+// the caller's face speed w is 0 (the face-list grids), so the face-speed terms are not built.
+template <typename T, int NSTATE, bool DELTA = false, bool MOVING = true>
 SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const double* q2d, int n_disc,
                           double* qqq, double* sp, int32_t* flag) {
     const double al = nrm[0], be = nrm[1], ge = nrm[2];
@@ -325,11 +326,11 @@ SB_HD void chlld_general(const double* nrm, double w, const double* q1d, const d
             fl = riemann<T, NSTATE, true, false>(a, b, T(w), n_disc, F, SL, SR, SM) | kFlagStar;
         }
     } else {
-        fl = riemann<T, NSTATE, true, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
+        fl = riemann<T, NSTATE, MOVING, (sizeof(T) == 4)>(a, b, T(w), n_disc, F, SL, SR, SM);
     }
     if (sizeof(T) == 4 && (fl & kFlagStar)) {
         // the mixed form's rule: a face whose FP32 star state is not positive is redone in FP64
-        chlld_general<double, NSTATE, false>(nrm, w, q1d, q2d, n_disc, qqq, sp, flag);
+        chlld_general<double, NSTATE, false, MOVING>(nrm, w, q1d, q2d, n_disc, qqq, sp, flag);
         *flag |= kFlagStar;
         return;
     }

@@ -100,11 +100,14 @@ def run_stream(requests, max_slots: int = 256, precision: int = 1, hbm_budget: i
 
 def solve_alone(inst, precision: int = 0, steady_tol: float = 1e-5, max_steps: int | None = None,
                 check_every: int = 50, keep_state: bool = False):
-    """One request by itself (a one-slot batch, same checks and stopping rule)."""
+    """One request by itself (a one-slot batch, same checks and stopping rule as the server: it
+    stops at the first check that finds it steady, past its cap, or failed; `status` is the
+    setb status the server would report)."""
     o = StepOpts()
     o.n_state, o.n_disc, o.order, o.scheme, o.precision, o.reserved, o.cfl = (
         inst.opts.n_state, inst.opts.n_disc, inst.opts.order, inst.opts.scheme, precision, 0, inst.opts.cfl)
     cap = max_steps if max_steps is not None else inst.steps
+    status = 0
     with Batch(1, precision=precision) as b:
         s = b.add(inst.desc, inst.ic, o)
         b.check()
@@ -113,12 +116,17 @@ def solve_alone(inst, precision: int = 0, steady_tol: float = 1e-5, max_steps: i
             b.step(check_every)
             steps += check_every
             last = b.check()[s]
+            try:
+                b.status(s)
+            except SetbError as e:
+                status = e.code
+                break
             if steady_tol > 0 and 0 <= last < steady_tol:
                 conv = True
                 break
         U = b.conserved(s) if keep_state else None
         d = b.status(s, check=False)
-    return {"steps": steps, "converged": conv, "last_change": last, "U": U, "diag": d}
+    return {"steps": steps, "converged": conv, "last_change": last, "U": U, "diag": d, "status": status}
 
 
 def run_sequential(requests, precision: int = 0, check_every: int = 50):
