@@ -201,17 +201,22 @@ __device__ __forceinline__ int riemann_f32x2(const float* q1, const float* q2, f
         const float sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
         ezz = right ? ez + pick(rzs, true) * sbn * (sbvS - sbzz) : ez - pick(rzs, false) * sbn * (sbvS - sbzz);
     }
-    const float Fs[8] = {m, (m * uu + pts) - bxs * bxs, m * vv - bxs * bys, m * ww - bxs * bzs,
-                         (e + pts) * uu - bxs * sbv, 0.0f, uu * bys - vv * bxs, uu * bzs - ww * bxs};
-    const float Us[8] = {rr, m, rr * vv, rr * ww, e, bxs, bys, bzs};
-    const float UZs[8] = {rzz, rzz * SM, rzz * v2s, rzz * v3s, ez, bn, b2z, b3z};
-    const float UZZs[8] = {rzz, rzz * SM, rzz * vzz2, rzz * vzz3, ezz, bn, bzz2, bzz3};
+    // the two tangential components of each vector, and the flux assembly, as f32x2 pairs
+    const F2 vw = mk(vv, ww), bt = mk(bys, bzs);
+    const F2 fs23 = fma2(splat(m), vw, splat(-bxs) * bt);   // m v - bx by, m w - bx bz
+    const F2 fs67 = fma2(splat(uu), bt, splat(-bxs) * vw);  // u by - v bx, u bz - w bx
+    const F2 us23 = splat(rr) * vw, uz23 = splat(rzz) * mk(v2s, v3s), uzz23 = splat(rzz) * mk(vzz2, vzz3);
+    const F2 Fs[4] = {mk(m, (m * uu + pts) - bxs * bxs), fs23, mk((e + pts) * uu - bxs * sbv, 0.0f), fs67};
+    const F2 Us[4] = {mk(rr, m), us23, mk(e, bxs), bt};
+    const F2 UZs[4] = {mk(rzz, rzz * SM), uz23, mk(ez, bn), mk(b2z, b3z)};
+    const F2 UZZs[4] = {mk(rzz, rzz * SM), uzz23, mk(ezz, bn), mk(bzz2, bzz3)};
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-        float f = Fs[k];
-        if (use2) f = f + S2 * (UZZs[k] - UZs[k]);
-        if (use1) f = f + S1 * (UZs[k] - Us[k]);
-        F[k] = f;
+    for (int k = 0; k < 4; k++) {
+        F2 f = Fs[k];
+        if (use2) f = fma2(splat(S2), UZZs[k] - UZs[k], f);
+        if (use1) f = fma2(splat(S1), UZs[k] - Us[k], f);
+        F[2 * k] = f.x;
+        F[2 * k + 1] = f.y;
     }
     if (use1) {   // positivity of the selected star state (rho* > 0, p* = pt* - |b*|^2/2 > 0)
         const float w6 = use2 ? bzz2 : b2z, w7 = use2 ? bzz3 : b3z;
@@ -222,9 +227,10 @@ __device__ __forceinline__ int riemann_f32x2(const float* q1, const float* q2, f
     F[5] = (-fmaxf(fabsf(SL), fabsf(SR)) * (bx.y - bx.x)) * spi4;
     F[6] *= spi4;
     F[7] *= spi4;
-#pragma unroll
-    for (int k = 0; k < 8; k++)
-        if (!(fabsf(F[k]) < 3.0e38f)) flag |= kFlagStar;
+    // a non-finite component makes the sum non-finite (finite physical fluxes are far below the
+    // FP32 range, so their sum cannot overflow): one test instead of eight
+    const F2 s2 = (mk(F[0], F[1]) + mk(F[2], F[3])) + (mk(F[4], F[5]) + mk(F[6], F[7]));
+    if (!(fabsf(s2.x + s2.y) < 3.0e38f)) flag |= kFlagStar;
     return flag;
 }
 

@@ -363,11 +363,14 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     const int lane = t & 31, warp = t >> 5;
     auto do_face = [&](int job, int k, bool dup) {
         int axis, fxx, fyy, gk, oidx, ostride;
+        double sq, idist;   // face area and 1/dist of the axis (compile-time index per branch)
         FT* out;
         bool real;
         RT qLL[8], qL[8], qR[8], qRR[8];
         if (job < JZ) {
             axis = 2;
+            sq = g.square[2];
+            idist = g.inv_dist[2];
             fxx = lane;
             fyy = job;
             const int c = (fyy + 2) * HX + fxx + 2;
@@ -381,6 +384,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             real = (i0 + fxx < g.nx) && (j0 + fyy < g.ny) && (k + 1 <= ke) && (k + 1 >= kb);
         } else if (job < JX) {
             axis = 0;
+            sq = g.square[0];
+            idist = g.inv_dist[0];
             if (job < 2 * TY) {
                 fxx = lane;
                 fyy = job - JZ;
@@ -399,6 +404,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             real = (i0 + fxx <= g.nx) && (j0 + fyy < g.ny);
         } else {
             axis = 1;
+            sq = g.square[1];
+            idist = g.inv_dist[1];
             fxx = lane;
             fyy = job - JX;
             const int c = fyy * HX + fxx + 2;     // row fyy-2 (tile-local)
@@ -413,7 +420,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         RT q1[8], q2[8], F[8];
         if constexpr (P == 1 && ORDER == 2) reconstruct_f32x2(qLL, qL, qR, qRR, q1, q2);
         else reconstruct<RT, ORDER>(qLL, qL, qR, qRR, q1, q2);
-        if (real && !dup && (q1[0] < RT(0) || q2[0] < RT(0))) n_recon++;
+        if (real && !dup && (sb_neg(q1[0]) || sb_neg(q2[0]))) n_recon++;
         int fl;
         double sl, sr;
         if constexpr (P == 2) {
@@ -444,7 +451,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
             sl = (double)SL;
             sr = (double)SR;
         }
-        const double sq = g.square[axis];
+
         if (P == 1 && real && (fl & kFlagStar)) {
             const FaceFlux r = face_fp64<NSTATE, ORDER>(fetch_args(A), axis, i0 + fxx, j0 + fyy, gk);
             fl = r.fl;
@@ -454,7 +461,9 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 #pragma unroll
             for (int v = 0; v < 8; v++) out[v * ostride + oidx] = (FT)(r.F[v] * sq);
         } else {
-            if (fl & kFlagWave) {
+            // a face no wave-fan region matched gets a zero flux; the warp vote keeps the (never
+            // taken in a valid state) zeroing out of the common path
+            if (__any_sync(__activemask(), fl & kFlagWave) && (fl & kFlagWave)) {
 #pragma unroll
                 for (int v = 0; v < 8; v++) F[v] = RT(0);
             }
@@ -465,7 +474,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
         if ((fl & kFlagWave) && real && !dup) n_wave++;
         // compare-and-select maxima (the library fmax of doubles is a far longer sequence); a NaN
         // speed is skipped, as fmax would skip it
-        if (WANT_DT && real) rate = sb_max(rate, sb_max(fabs(sl), fabs(sr)) * g.inv_dist[axis]);
+        if (WANT_DT && real) rate = sb_max(rate, sb_max(fabs(sl), fabs(sr)) * idist);
     };
 
     // ---- the march over planes kk = k0-2 .. k1+1.  Plane kk enters ring slot kk; from
