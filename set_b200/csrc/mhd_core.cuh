@@ -97,9 +97,9 @@ SB_HD float sb_rsqrt(float x) {
 // positive normal x whose result is normal (the approximate instructions flush subnormals);
 // there 1/x and 1/sqrt(x) are within one ulp and sqrt(x) within two, mostly correctly rounded
 // (tests/test_gpu_special.py checks 2^20 inputs over 1e-300..1e300).  At 0 and +-inf 1/x and
-// 1/sqrt(x) give NaN; at subnormals 1/x gives NaN and 1/sqrt(x) +inf (sqrt(0) = 0).  Every argument the flux passes them is a positive density, a sum of squares
-// under sb_pos, or a wave-speed difference that a valid state keeps away from zero (SR - SL >=
-// cfL + cfR > 0; the star denominators tt are screened against 1e-9 before the reciprocal); a
+// 1/sqrt(x) give NaN; at subnormals 1/x gives NaN and 1/sqrt(x) +inf (sqrt(0) = 0).  Every
+// argument the flux passes them is a positive density, a sum of squares under sb_pos, or a
+// wave-speed difference that a valid state keeps away from zero (SR - SL >= cfL + cfR > 0; the star denominators tt are screened against 1e-9 before the reciprocal); a
 // state that is already invalid (rho <= 0) is reported by the cell update's counters either way.
 // Three (1/x), five (1/sqrt(x)) and six (sqrt(x)) FP64 operations after the seed: fewer than the
 // correctly rounded library forms, on the pipe that bounds the plain form; the state conversions,
