@@ -295,6 +295,23 @@ SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
 constexpr double kPFloorE = kPFloor / kG1;
 SB_HD double floor_energy(double ke, double me) { return rn_add(rn_add(kPFloorE, ke), me); }
 
+// A sufficient test that the exact recovery's pressure, ((E - ke) - me)(gamma - 1), is positive,
+// at a third of its cost.  X' = (E - |m|^2/(2 rho)) - |B|^2/(8 pi) with a reciprocal of one ulp
+// differs from the exact recovery's (E - ke) - me by at most ~17 units of 2^-53 times
+// |E| + ke + me (ke, me carry at most 6-7 roundings each, X' at most 7; two subtractions
+// each), so X' above 2^-48 (|E| + ke' + me') -- plus 1e-300 against subnormal magnitudes -- means
+// the exact pressure is positive and the pressure floor does not apply.  Otherwise the caller
+// runs the exact recovery.
+SB_HD bool pressure_surely_positive(const double* U) {
+    const double ir = rs_rcp(U[0]);
+    const double m2 = (U[1] * U[1] + U[2] * U[2]) + U[3] * U[3];
+    const double b2 = (U[5] * U[5] + U[6] * U[6]) + U[7] * U[7];
+    const double ke = 0.5 * m2 * ir;
+    const double me = b2 * (0.5 * kInvSpi4 * kInvSpi4);
+    const double x = (U[4] - ke) - me;
+    return x > 0x1p-48 * ((sb_abs(U[4]) + ke) + me) + 1e-300;
+}
+
 // ------------------------------------------------------------------ Riemann solver
 // Face-frame states q = (rho, vn, vt1, vt2, p, Bn, Bt1, Bt2), B in stored units.
 // Output F in the same order (B fluxes in stored units, not multiplied by the face area),
@@ -302,7 +319,11 @@ SB_HD double floor_energy(double ke, double me) { return rn_add(rn_add(kPFloorE,
 // Returns a bit set: kFlagWave when no wave-fan region matched (the reference STOPs),
 // kFlagStar (CHECK_STAR only) when the selected state has rho <= 0 or p <= 0 or F is not finite.
 // BS: the states carry b = B / sqrt(4 pi) already (q[5..7]), so the solver skips its scaling.
-template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR, bool NR = true, bool BS = false>
+// LAZY (HLLC / HLLD): skip what the selected wave-fan region does not read (the FP64 stage
+// kernels); !LAZY evaluates every region's quantities branch-free and selects, which needs fewer
+// registers where the solver is a rare path of a kernel whose register budget it would set.
+template <typename T, int NSTATE, bool MOVING, bool CHECK_STAR, bool NR = true, bool BS = false,
+          bool LAZY = true>
 SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& SRo, T& SMo) {
     const T ispi4 = T(kInvSpi4);
     const T ga = T(kGamma);
@@ -369,11 +390,8 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
     }
 
     int flag = 0;
-    const T isrl = fr_rcp<NR>(SR - SL);
-    // HLL average of the normal field, UZ(6) (:1406-1408 with FL(6) = FR(6) = 0)
-    const T bn = (SR * bx2 - SL * bx1) * isrl;
-
     if (NSTATE <= 1) {   // :1414-1463, with the left/right energies, fluxes and states of :1368-1404
+        const T isrl = fr_rcp<NR>(SR - SL);
         const T e1 = (p1 * ig1 + r1 * (half * ((u1 * u1 + v1 * v1) + w1 * w1))) + half * b2L;
         const T e2 = (p2 * ig1 + r2 * (half * ((u2 * u2 + v2 * v2) + w2 * w2))) + half * b2R;
         const T sbv1 = (u1 * bx1 + v1 * by1) + w1 * bz1;
@@ -420,115 +438,63 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         }
         if (!(SL > wv) && !(SL <= wv && wv <= SR) && !(SR < wv)) flag |= kFlagWave;
     } else {
-        // The wave-fan region needs only SL, SR, SM and the star densities, so it is found first
-        // and the energy, physical flux and conserved vector (:1368-1404) and the star energy are
-        // formed for the selected side alone.
-        const T isrm = fr_rcp<NR>(SR - SM), islm = fr_rcp<NR>(SL - SM);
-        const T suRm = suR * isrm, suLm = suL * islm;
-        const T rzR = r2 * suRm, rzL = r1 * suLm;
-        T vzL2, vzL3, vzR2, vzR3, bzL2, bzL3, bzR2, bzR3;
-        int region;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
-        T vzz2 = T(0), vzz3 = T(0), bzz2 = T(0), bzz3 = T(0);
-        T SZL = SM, SZR = SM;
-        T ptz;        // total pressure of the star states
-        T sbvz = T(0), rzRs = T(0), rzLs = T(0), sbn = T(0);
+        // The wave-fan region is found first and (LAZY) everything else is formed only where the
+        // selected region reads it.  The region chains of :1521-1567 and :1722-1814 (last match
+        // wins) end with FR (SR < wv), so SR < wv selects FR whatever the other speeds are: no HLL
+        // average, star density or Alfven speed is needed there.  FL (SL > wv) holds only when no later region
+        // matches, so it is decided with the others.  The star states (:1465-1567 / :1598-1718)
+        // and the star energy are formed for the star regions alone, a side's single-star state
+        // for the regions that read it; the energy, physical flux and conserved vector
+        // (:1368-1404) for the selected side alone.
+        int region = 6;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
+        T isrl = T(0), bn = T(0), isrm = T(0), islm = T(0), suRm = T(0), suLm = T(0), rzR = T(0), rzL = T(0);
+        T rzRs = T(0), rzLs = T(0), sbn = T(0), SZL = SM, SZR = SM;
+        T isR = T(0), isL = T(0);
         bool ibn = false;
-        if (NSTATE == 2) {   // HLLC, :1465-1567
-            ptz = half * ((ptR + r2 * suR * (SM - u2)) + (ptL + r1 * suL * (SM - u1)));
-            const T m1 = r1 * u1, m2 = r2 * u2;
-            const T FL1 = (m1 * u1 + ptL) - bx1 * bx1, FR1 = (m2 * u2 + ptR) - bx2 * bx2;
-            const T FL2 = m1 * v1 - bx1 * by1, FR2 = m2 * v2 - bx2 * by2;
-            const T FL3 = m1 * w1 - bx1 * bz1, FR3 = m2 * w2 - bx2 * bz2;
-            const T FL6 = u1 * by1 - v1 * bx1, FR6 = u2 * by2 - v2 * bx2;
-            const T FL7 = u1 * bz1 - w1 * bx1, FR7 = u2 * bz2 - w2 * bx2;
-            const T uz0 = ((SR * r2 - SL * r1) + m1 - m2) * isrl;
-            const T uz1 = ((SR * m2 - SL * m1) + FL1 - FR1) * isrl;
-            const T uz2 = ((SR * (r2 * v2) - SL * (r1 * v1)) + FL2 - FR2) * isrl;
-            const T uz3 = ((SR * (r2 * w2) - SL * (r1 * w1)) + FL3 - FR3) * isrl;
-            const T uz6 = ((SR * by2 - SL * by1) + FL6 - FR6) * isrl;
-            const T uz7 = ((SR * bz2 - SL * bz1) + FL7 - FR7) * isrl;
-            sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * fr_rcp<NR>(uz0);
-            if (sb_abs(bn) < T(kEpsB)) {
-                vzR2 = v2; vzR3 = w2; vzL2 = v1; vzL3 = w1;
-                bzR2 = by2 * suRm; bzR3 = bz2 * suRm;
-                bzL2 = by1 * suLm; bzL3 = bz1 * suLm;
-            } else {
-                const T cR = bn * fr_rcp<NR>(suR * r2), cL = bn * fr_rcp<NR>(suL * r1);
-                vzR2 = v2 + (by2 - uz6) * cR;
-                vzR3 = w2 + (bz2 - uz7) * cR;
-                vzL2 = v1 + (by1 - uz6) * cL;
-                vzL3 = w1 + (bz1 - uz7) * cL;
-                bzR2 = uz6; bzR3 = uz7; bzL2 = uz6; bzL3 = uz7;
-            }
-            if (SR < wv) region = 6;
-            else if (SM <= wv && SR >= wv) region = 5;
-            else if (SL <= wv && SM >= wv) region = 2;
-            else if (SL > wv) region = 1;
-            else region = 0;
-        } else {             // HLLD, :1598-1814
-            ptz = ((suR * r2 * ptL - suL * r1 * ptR) + r1 * r2 * suR * suL * (u2 - u1)) * idd;
-            const T bn2 = bn * bn;
-            T tvR = T(0), tbR = T(0), tvL = T(0), tbL = T(0);
-            const T ttR = r2 * suR * (SR - SM) - bn2;
-            if (!(sb_abs(ttR) <= T(kTtEps))) {
-                const T i = fr_rcp<NR>(ttR);
-                tvR = (SM - u2) * i;
-                tbR = (r2 * suR * suR - bn2) * i;
-            }
-            const T ttL = r1 * suL * (SL - SM) - bn2;
-            if (!(sb_abs(ttL) <= T(kTtEps))) {
-                const T i = fr_rcp<NR>(ttL);
-                tvL = (SM - u1) * i;
-                tbL = (r1 * suL * suL - bn2) * i;
-            }
-            vzL2 = v1 - bn * by1 * tvL;
-            vzL3 = w1 - bn * bz1 * tvL;
-            vzR2 = v2 - bn * by2 * tvR;
-            vzR3 = w2 - bn * bz2 * tvR;
-            bzL2 = by1 * tbL;
-            bzL3 = bz1 * tbL;
-            bzR2 = by2 * tbR;
-            bzR3 = bz2 * tbR;
-            const T isR = fr_rsqrt<NR>(rzR), isL = fr_rsqrt<NR>(rzL);   // 1/sqrt(rho*) and sqrt(rho*) = rho*/sqrt(rho*)
-            rzRs = rzR * isR;
-            rzLs = rzL * isL;
-            const T abn = sb_abs(bn);
-            if (abn > T(kEpsB)) {
-                ibn = true;
-                sbn = bn > T(0) ? T(1) : T(-1);
-                SZL = SM - abn * isL;
-                SZR = SM + abn * isR;
-            }
-            if (SR < wv) region = 6;
-            else if (SZR <= wv && SR >= wv) region = 5;
-            else if (ibn && SM <= wv && SZR >= wv) region = 4;
-            else if (ibn && SZL <= wv && SM >= wv) region = 3;
-            else if (SL <= wv && SZL >= wv) region = 2;
-            else if (SL > wv) region = 1;
-            else region = 0;
-            if (region == 3 || region == 4) {
-                const T irzss = fr_rcp<NR>(rzRs + rzLs);
-                const T rzps = rzRs * rzLs;
-                vzz2 = ((rzLs * vzL2 + rzRs * vzR2) + sbn * (bzR2 - bzL2)) * irzss;
-                vzz3 = ((rzLs * vzL3 + rzRs * vzR3) + sbn * (bzR3 - bzL3)) * irzss;
-                bzz2 = ((rzLs * bzR2 + rzRs * bzL2) + sbn * rzps * (vzR2 - vzL2)) * irzss;
-                bzz3 = ((rzLs * bzR3 + rzRs * bzL3) + sbn * rzps * (vzR3 - vzL3)) * irzss;
+        if (!LAZY || !(SR < wv)) {
+            isrl = fr_rcp<NR>(SR - SL);
+            bn = (SR * bx2 - SL * bx1) * isrl;   // HLL average of the normal field, UZ(6) (:1406-1408)
+            isrm = fr_rcp<NR>(SR - SM);
+            islm = fr_rcp<NR>(SL - SM);
+            suRm = suR * isrm;
+            suLm = suL * islm;
+            rzR = r2 * suRm;
+            rzL = r1 * suLm;
+            if (NSTATE == 2) {   // HLLC, :1521-1567
+                if (SR < wv) region = 6;
+                else if (SM <= wv && SR >= wv) region = 5;
+                else if (SL <= wv && SM >= wv) region = 2;
+                else if (SL > wv) region = 1;
+                else region = 0;
+            } else {             // HLLD, :1660-1676, :1722-1814
+                isR = fr_rsqrt<NR>(rzR);   // 1/sqrt(rho*) and sqrt(rho*) = rho*/sqrt(rho*)
+                isL = fr_rsqrt<NR>(rzL);
+                rzRs = rzR * isR;
+                rzLs = rzL * isL;
+                const T abn = sb_abs(bn);
+                if (abn > T(kEpsB)) {
+                    ibn = true;
+                    sbn = bn > T(0) ? T(1) : T(-1);
+                    SZL = SM - abn * isL;
+                    SZR = SM + abn * isR;
+                }
+                if (SR < wv) region = 6;
+                else if (SZR <= wv && SR >= wv) region = 5;
+                else if (ibn && SM <= wv && SZR >= wv) region = 4;
+                else if (ibn && SZL <= wv && SM >= wv) region = 3;
+                else if (SL <= wv && SZL >= wv) region = 2;
+                else if (SL > wv) region = 1;
+                else region = 0;
             }
         }
         if (region == 0) flag |= kFlagWave;
         const bool right = region >= 4;
-        const bool use1 = (region == 2 || region == 3 || region == 4 || region == 5);
+        const bool use1 = (region >= 2 && region <= 5);
         const bool use2 = (region == 3 || region == 4);
         // the selected side
         const T r = right ? r2 : r1, u = right ? u2 : u1, v = right ? v2 : v1, w = right ? w2 : w1;
         const T p = right ? p2 : p1, bx = right ? bx2 : bx1, by = right ? by2 : by1, bz = right ? bz2 : bz1;
         const T pt = right ? ptR : ptL, b2 = right ? b2R : b2L;
-        const T sum = right ? suRm : suLm, ism = right ? isrm : islm;
-        const T rz = right ? rzR : rzL;
-        const T S1 = right ? SR : SL;
-        const T S2 = right ? SZR : SZL;
-        const T vz2 = right ? vzR2 : vzL2, vz3 = right ? vzR3 : vzL3;
-        const T bz2_ = right ? bzR2 : bzL2, bz3_ = right ? bzR3 : bzL3;
         const T e = (p * ig1 + r * (half * ((u * u + v * v) + w * w))) + half * b2;
         const T sbv = (u * bx + v * by) + w * bz;
         const T m = r * u;
@@ -543,36 +509,122 @@ SB_HD int riemann(const T* q1, const T* q2, T wv, int n_disc, T* F, T& SLo, T& S
         Fs[7] = u * bz - w * bx;
         Us[0] = r; Us[1] = m; Us[2] = r * v; Us[3] = r * w; Us[4] = e;
         Us[5] = bx; Us[6] = by; Us[7] = bz;
-        // star energy of the selected side (:1541-1544 / :1650-1656) and its double star
-        // (:1710-1718)
-        const T sbvS = NSTATE == 2 ? sbvz : (bn * SM + bz2_ * vz2) + bz3_ * vz3;
-        const T ez = e * sum + (((ptz * SM - pt * u) + bn * (sbv - sbvS)) * ism);
-        T ezz = ez;
-        if (NSTATE == 3 && use2) {
-            const T sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
-            ezz = right ? ez + rzRs * sbn * (sbvS - sbzz) : ez - rzLs * sbn * (sbvS - sbzz);
-        }
-        T UZs[8], UZZs[8];
-        UZs[0] = rz; UZs[1] = rz * SM; UZs[2] = rz * vz2; UZs[3] = rz * vz3; UZs[4] = ez;
-        UZs[5] = bn; UZs[6] = bz2_; UZs[7] = bz3_;
-        UZZs[0] = rz; UZZs[1] = rz * SM; UZZs[2] = rz * vzz2; UZZs[3] = rz * vzz3; UZZs[4] = ezz;
-        UZZs[5] = bn; UZZs[6] = bzz2; UZZs[7] = bzz3;
         T W[8];   // the state whose flux is returned (for the face-speed term and the check)
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-            T f = Fs[k];
-            if (use2) f = f + S2 * (UZZs[k] - UZs[k]);
-            if (use1) f = f + S1 * (UZs[k] - Us[k]);
-            W[k] = use2 ? UZZs[k] : (use1 ? UZs[k] : Us[k]);
-            if (MOVING) f = f - wv * W[k];
-            F[k] = f;
+            F[k] = Fs[k];
+            W[k] = Us[k];
         }
-        if (CHECK_STAR && use1) {
-            // positivity of the selected star state: rho* > 0 and p* = pt* - |b*|^2/2 > 0 (the
-            // gas pressure from the star total pressure avoids the kinetic-energy cancellation
-            // of E - rho|v|^2/2); FL / FR themselves are the reconstructed, positive states
-            const T bb = (bn * bn + W[6] * W[6]) + W[7] * W[7];
-            if (!(rz > T(0)) || !(ptz - half * bb > T(0))) flag |= kFlagStar;
+        if (!LAZY || use1) {
+            T vzL2 = T(0), vzL3 = T(0), vzR2 = T(0), vzR3 = T(0);
+            T bzL2 = T(0), bzL3 = T(0), bzR2 = T(0), bzR3 = T(0);
+            T vzz2 = T(0), vzz3 = T(0), bzz2 = T(0), bzz3 = T(0);
+            T ptz;        // total pressure of the star states
+            T sbvz = T(0);
+            if (NSTATE == 2) {   // HLLC, :1465-1558
+                ptz = half * ((ptR + r2 * suR * (SM - u2)) + (ptL + r1 * suL * (SM - u1)));
+                const T m1 = r1 * u1, m2 = r2 * u2;
+                const T FL1 = (m1 * u1 + ptL) - bx1 * bx1, FR1 = (m2 * u2 + ptR) - bx2 * bx2;
+                const T FL2 = m1 * v1 - bx1 * by1, FR2 = m2 * v2 - bx2 * by2;
+                const T FL3 = m1 * w1 - bx1 * bz1, FR3 = m2 * w2 - bx2 * bz2;
+                const T FL6 = u1 * by1 - v1 * bx1, FR6 = u2 * by2 - v2 * bx2;
+                const T FL7 = u1 * bz1 - w1 * bx1, FR7 = u2 * bz2 - w2 * bx2;
+                const T uz0 = ((SR * r2 - SL * r1) + m1 - m2) * isrl;
+                const T uz1 = ((SR * m2 - SL * m1) + FL1 - FR1) * isrl;
+                const T uz2 = ((SR * (r2 * v2) - SL * (r1 * v1)) + FL2 - FR2) * isrl;
+                const T uz3 = ((SR * (r2 * w2) - SL * (r1 * w1)) + FL3 - FR3) * isrl;
+                const T uz6 = ((SR * by2 - SL * by1) + FL6 - FR6) * isrl;
+                const T uz7 = ((SR * bz2 - SL * bz1) + FL7 - FR7) * isrl;
+                sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * fr_rcp<NR>(uz0);
+                if (sb_abs(bn) < T(kEpsB)) {
+                    vzR2 = v2; vzR3 = w2; vzL2 = v1; vzL3 = w1;
+                    bzR2 = by2 * suRm; bzR3 = bz2 * suRm;
+                    bzL2 = by1 * suLm; bzL3 = bz1 * suLm;
+                } else {
+                    const T cR = bn * fr_rcp<NR>(suR * r2), cL = bn * fr_rcp<NR>(suL * r1);
+                    vzR2 = v2 + (by2 - uz6) * cR;
+                    vzR3 = w2 + (bz2 - uz7) * cR;
+                    vzL2 = v1 + (by1 - uz6) * cL;
+                    vzL3 = w1 + (bz1 - uz7) * cL;
+                    bzR2 = uz6; bzR3 = uz7; bzL2 = uz6; bzL3 = uz7;
+                }
+            } else {             // HLLD, :1598-1718
+                ptz = ((suR * r2 * ptL - suL * r1 * ptR) + r1 * r2 * suR * suL * (u2 - u1)) * idd;
+                const T bn2 = bn * bn;
+                if (!LAZY || region <= 4) {   // L*, L**, R**: the left single-star state
+                    T tvL = T(0), tbL = T(0);
+                    const T ttL = r1 * suL * (SL - SM) - bn2;
+                    if (!(sb_abs(ttL) <= T(kTtEps))) {
+                        const T i = fr_rcp<NR>(ttL);
+                        tvL = (SM - u1) * i;
+                        tbL = (r1 * suL * suL - bn2) * i;
+                    }
+                    vzL2 = v1 - bn * by1 * tvL;
+                    vzL3 = w1 - bn * bz1 * tvL;
+                    bzL2 = by1 * tbL;
+                    bzL3 = bz1 * tbL;
+                }
+                if (!LAZY || region >= 3) {   // L**, R**, R*: the right single-star state
+                    T tvR = T(0), tbR = T(0);
+                    const T ttR = r2 * suR * (SR - SM) - bn2;
+                    if (!(sb_abs(ttR) <= T(kTtEps))) {
+                        const T i = fr_rcp<NR>(ttR);
+                        tvR = (SM - u2) * i;
+                        tbR = (r2 * suR * suR - bn2) * i;
+                    }
+                    vzR2 = v2 - bn * by2 * tvR;
+                    vzR3 = w2 - bn * bz2 * tvR;
+                    bzR2 = by2 * tbR;
+                    bzR3 = bz2 * tbR;
+                }
+                if (use2) {
+                    const T irzss = fr_rcp<NR>(rzRs + rzLs);
+                    const T rzps = rzRs * rzLs;
+                    vzz2 = ((rzLs * vzL2 + rzRs * vzR2) + sbn * (bzR2 - bzL2)) * irzss;
+                    vzz3 = ((rzLs * vzL3 + rzRs * vzR3) + sbn * (bzR3 - bzL3)) * irzss;
+                    bzz2 = ((rzLs * bzR2 + rzRs * bzL2) + sbn * rzps * (vzR2 - vzL2)) * irzss;
+                    bzz3 = ((rzLs * bzR3 + rzRs * bzL3) + sbn * rzps * (vzR3 - vzL3)) * irzss;
+                }
+            }
+            const T sum = right ? suRm : suLm, ism = right ? isrm : islm;
+            const T rz = right ? rzR : rzL;
+            const T S1 = right ? SR : SL;
+            const T S2 = right ? SZR : SZL;
+            const T vz2 = right ? vzR2 : vzL2, vz3 = right ? vzR3 : vzL3;
+            const T bz2_ = right ? bzR2 : bzL2, bz3_ = right ? bzR3 : bzL3;
+            // star energy of the selected side (:1541-1544 / :1650-1656) and its double star
+            // (:1710-1718)
+            const T sbvS = NSTATE == 2 ? sbvz : (bn * SM + bz2_ * vz2) + bz3_ * vz3;
+            const T ez = e * sum + (((ptz * SM - pt * u) + bn * (sbv - sbvS)) * ism);
+            T ezz = ez;
+            if (NSTATE == 3 && use2) {
+                const T sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
+                ezz = right ? ez + rzRs * sbn * (sbvS - sbzz) : ez - rzLs * sbn * (sbvS - sbzz);
+            }
+            T UZs[8], UZZs[8];
+            UZs[0] = rz; UZs[1] = rz * SM; UZs[2] = rz * vz2; UZs[3] = rz * vz3; UZs[4] = ez;
+            UZs[5] = bn; UZs[6] = bz2_; UZs[7] = bz3_;
+            UZZs[0] = rz; UZZs[1] = rz * SM; UZZs[2] = rz * vzz2; UZZs[3] = rz * vzz3; UZZs[4] = ezz;
+            UZZs[5] = bn; UZZs[6] = bzz2; UZZs[7] = bzz3;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                T f = Fs[k];
+                if (use2) f = f + S2 * (UZZs[k] - UZs[k]);
+                if (LAZY || use1) f = f + S1 * (UZs[k] - Us[k]);
+                W[k] = use2 ? UZZs[k] : (LAZY || use1 ? UZs[k] : Us[k]);
+                F[k] = f;
+            }
+            if (CHECK_STAR && (LAZY || use1)) {
+                // positivity of the selected star state: rho* > 0 and p* = pt* - |b*|^2/2 > 0 (the
+                // gas pressure from the star total pressure avoids the kinetic-energy cancellation
+                // of E - rho|v|^2/2); FL / FR themselves are the reconstructed, positive states
+                const T bb = (bn * bn + W[6] * W[6]) + W[7] * W[7];
+                if (!(rz > T(0)) || !(ptz - half * bb > T(0))) flag |= kFlagStar;
+            }
+        }
+        if (MOVING) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) F[k] = F[k] - wv * W[k];
         }
         // normal-field flux, :1570-1581 / :1828-1839
         const T SN = sb_max(sb_abs(SL), sb_abs(SR));

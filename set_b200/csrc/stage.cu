@@ -277,7 +277,7 @@ __device__ __noinline__ FaceFlux face_fp64(const FetchArgs fa, int axis, int i, 
     double q1[8], q2[8], G[8], SM;
     reconstruct<double, ORDER>(f[0], f[1], f[2], f[3], q1, q2);
     FaceFlux r;
-    r.fl = riemann<double, NSTATE, false, false, false>(q1, q2, 0.0, fa.n_disc, G, r.sl, r.sr, SM);
+    r.fl = riemann<double, NSTATE, false, false, false, false, false>(q1, q2, 0.0, fa.n_disc, G, r.sl, r.sr, SM);
     for (int v = 0; v < 8; v++) r.F[perm[v]] = G[v];
     return r;
 }
@@ -337,6 +337,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
     const int k0 = kb + bz * g.lz;
     const int k1 = min(ke, k0 + g.lz);
     const double dt = A.clk->dt_cur;
+    const double dt_vol = dt * g.inv_vol;   // dt / cell volume
     if (t < 6) cnt[t] = 0;
 
     double rate = 0.0;   // max over this thread's real faces of max(|SL|,|SR|)/dist
@@ -443,7 +444,7 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                 if (A.n_disc == 0)
                     fl = riemann_f32x2<NSTATE>(q1, q2, F, SL, SR, SM);
                 else
-                    fl = riemann<RT, NSTATE, false, true>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
+                    fl = riemann<RT, NSTATE, false, true, true, false, false>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
             } else {
                 // the plain form's ring holds b = B / sqrt(4 pi) (BS)
                 fl = riemann<RT, NSTATE, false, P == 1, true, P == 0>(q1, q2, RT(0), A.n_disc, F, SL, SR, SM);
@@ -572,16 +573,16 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
                         const float ay = fy[v * NYF + (ty + 1) * TX + tx] - fy[v * NYF + ty * TX + tx];
                         pot = (double)((ax + ay) + (fzh[v] - fzl[v]));
                     } else {
-                        pot = 0.0;
-                        pot = pot - (double)fx[v * NXF + ty * (TX + 1) + tx];
-                        pot = pot + (double)fx[v * NXF + ty * (TX + 1) + tx + 1];
+                        // the oracle's sum from zero, 0 - a + b - ...: (0 - a) + b equals b - a
+                        // bit for bit, zero signs included
+                        pot = (double)fx[v * NXF + ty * (TX + 1) + tx + 1] - (double)fx[v * NXF + ty * (TX + 1) + tx];
                         pot = pot - (double)fy[v * NYF + ty * TX + tx];
                         pot = pot + (double)fy[v * NYF + (ty + 1) * TX + tx];
                         pot = pot - (double)fzl[v];
                         pot = pot + (double)fzh[v];
                     }
                     uin[v] = A.Uin[v * g.vs + off];
-                    const double inc = dt * (pot * g.inv_vol);
+                    const double inc = pot * dt_vol;
                     if (P != 0 && A.comp) {
                         // compensated sum U_new = base + delta (cuf_solvers.cuf:741-770 as an
                         // increment); the FP32 compensation carries the rounding of the add
@@ -604,7 +605,8 @@ __device__ __forceinline__ void run_tile(const StageArgs& A, int bx, int by, int
 #pragma unroll
                     for (int v = 0; v < 8; v++) un[v] = uin[v];
                     reset_comp = true;
-                } else {
+                } else if (P == 1 || !pressure_surely_positive(un)) {
+                    // the exact recovery (P != 1) only where the quick test cannot clear p > 0
                     double q[8], ke, me;
                     prim_from_cons<P != 1>(un, q, ke, me);
                     if (q[4] <= 0.0) {                    // cuf_solvers.cuf:777-779
