@@ -93,134 +93,147 @@ __device__ __forceinline__ int riemann_f32x2(const float* q1, const float* q2, f
     SRo = SR;
     SMo = SM;
 
-    const float isrl = sb_rcp(SR - SL);
-    const float bn = (SR * bx.y - SL * bx.x) * isrl;   // HLL average of the normal field
-    const F2 sm = S - splat(SM);                       // (SL - SM, SR - SM)
-    const F2 ism = rcp2(sm);
-    const F2 sum = su * ism;
-    const F2 rz = r * sum;                             // star densities
-
-    F2 vz2, vz3, bz2, bz3;                             // star tangential velocity / field
+    // The wave-fan region first (FR, SR < 0, is the last match of the region chain and needs none
+    // of the star quantities); the star states and energies only for the star regions.
+    float bn = 0.0f;
+    F2 ism = splat(0.0f), sum = splat(0.0f), rz = splat(0.0f);
+    F2 vz2 = splat(0.0f), vz3 = splat(0.0f);           // star tangential velocity
+    F2 bz2 = splat(0.0f), bz3 = splat(0.0f);           // star tangential field
     F2 rzs = splat(0.0f);                              // sqrt(rho*)
-    float ptz, sbvz = 0.0f, sbn = 0.0f, SZL = SM, SZR = SM;
+    float ptz = 0.0f, sbvz = 0.0f, sbn = 0.0f, SZL = SM, SZR = SM;
     bool ibn = false;
-    int region;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
-    if (NSTATE == 2) {   // HLLC (:1465-1567)
-        const F2 smu = splat(SM) - u;
-        const F2 pzs = fma2(rsu, smu, pt);                // pt + r su (SM - u)
-        ptz = half * (pzs.y + pzs.x);
-        const F2 m = r * u;
-        const F2 f1 = fma2(m, u, pt) - bxx, f2 = m * v - bx * by, f3 = m * w - bx * bz;
-        const F2 f6 = u * by - v * bx, f7 = u * bz - w * bx;
-        const F2 rv = r * v, rw = r * w;
-        const float uz0 = ((SR * r.y - SL * r.x) + m.x - m.y) * isrl;
-        const float uz1 = ((SR * m.y - SL * m.x) + f1.x - f1.y) * isrl;
-        const float uz2 = ((SR * rv.y - SL * rv.x) + f2.x - f2.y) * isrl;
-        const float uz3 = ((SR * rw.y - SL * rw.x) + f3.x - f3.y) * isrl;
-        const float uz6 = ((SR * by.y - SL * by.x) + f6.x - f6.y) * isrl;
-        const float uz7 = ((SR * bz.y - SL * bz.x) + f7.x - f7.y) * isrl;
-        sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * sb_rcp(uz0);
-        if (fabsf(bn) < (float)kEpsB) {
-            vz2 = v;
-            vz3 = w;
-            bz2 = by * sum;
-            bz3 = bz * sum;
-        } else {
-            const F2 c = splat(bn) * rcp2(rsu);
-            vz2 = fma2(by - splat(uz6), c, v);
-            vz3 = fma2(bz - splat(uz7), c, w);
-            bz2 = splat(uz6);
-            bz3 = splat(uz7);
+    int region = 6;   // 1: FL, 2: L*, 3: L**, 4: R**, 5: R*, 6: FR, 0: none
+    if (!(SR < 0.0f)) {
+        const float isrl = sb_rcp(SR - SL);
+        bn = (SR * bx.y - SL * bx.x) * isrl;   // HLL average of the normal field
+        const F2 sm = S - splat(SM);                       // (SL - SM, SR - SM)
+        ism = rcp2(sm);
+        sum = su * ism;
+        rz = r * sum;                                     // star densities
+        if (NSTATE == 2) {   // HLLC (:1465-1567)
+            const F2 smu = splat(SM) - u;
+            const F2 pzs = fma2(rsu, smu, pt);                // pt + r su (SM - u)
+            ptz = half * (pzs.y + pzs.x);
+            const F2 m = r * u;
+            const F2 f1 = fma2(m, u, pt) - bxx, f2 = m * v - bx * by, f3 = m * w - bx * bz;
+            const F2 f6 = u * by - v * bx, f7 = u * bz - w * bx;
+            const F2 rv = r * v, rw = r * w;
+            const float uz0 = ((SR * r.y - SL * r.x) + m.x - m.y) * isrl;
+            const float uz1 = ((SR * m.y - SL * m.x) + f1.x - f1.y) * isrl;
+            const float uz2 = ((SR * rv.y - SL * rv.x) + f2.x - f2.y) * isrl;
+            const float uz3 = ((SR * rw.y - SL * rw.x) + f3.x - f3.y) * isrl;
+            const float uz6 = ((SR * by.y - SL * by.x) + f6.x - f6.y) * isrl;
+            const float uz7 = ((SR * bz.y - SL * bz.x) + f7.x - f7.y) * isrl;
+            sbvz = ((bn * uz1 + uz6 * uz2) + uz7 * uz3) * sb_rcp(uz0);
+            if (fabsf(bn) < (float)kEpsB) {
+                vz2 = v;
+                vz3 = w;
+                bz2 = by * sum;
+                bz3 = bz * sum;
+            } else {
+                const F2 c = splat(bn) * rcp2(rsu);
+                vz2 = fma2(by - splat(uz6), c, v);
+                vz3 = fma2(bz - splat(uz7), c, w);
+                bz2 = splat(uz6);
+                bz3 = splat(uz7);
+            }
+            if (SR < 0.0f) region = 6;
+            else if (SM <= 0.0f && SR >= 0.0f) region = 5;
+            else if (SL <= 0.0f && SM >= 0.0f) region = 2;
+            else if (SL > 0.0f) region = 1;
+            else region = 0;
+        } else {             // HLLD (:1598-1814)
+            const F2 rsupt = rsu * mk(pt.y, pt.x);           // (suL r1 ptR, suR r2 ptL)
+            ptz = ((rsupt.y - rsupt.x) + r.x * r.y * su.y * su.x * (u.y - u.x)) * idd;
+            const float bn2 = bn * bn;
+            const F2 tt = rsu * sm - splat(bn2);             // r su (S - SM) - bn^2
+            const F2 itt = rcp2(tt);
+            const bool degL = fabsf(tt.x) <= (float)kTtEps, degR = fabsf(tt.y) <= (float)kTtEps;
+            F2 tv = (splat(SM) - u) * itt;
+            F2 tb = fma2(rsu, su, splat(-bn2)) * itt;        // (r su^2 - bn^2) / tt
+            if (degL) tv.x = tb.x = 0.0f;
+            if (degR) tv.y = tb.y = 0.0f;
+            const F2 nbn = splat(-bn);
+            vz2 = fma2(nbn, by * tv, v);
+            vz3 = fma2(nbn, bz * tv, w);
+            bz2 = by * tb;
+            bz3 = bz * tb;
+            const F2 isq = rsqrt2(rz);
+            rzs = rz * isq;
+            const float abn = fabsf(bn);
+            if (abn > (float)kEpsB) {
+                ibn = true;
+                sbn = bn > 0.0f ? 1.0f : -1.0f;
+                SZL = SM - abn * isq.x;
+                SZR = SM + abn * isq.y;
+            }
+            if (SR < 0.0f) region = 6;
+            else if (SZR <= 0.0f && SR >= 0.0f) region = 5;
+            else if (ibn && SM <= 0.0f && SZR >= 0.0f) region = 4;
+            else if (ibn && SZL <= 0.0f && SM >= 0.0f) region = 3;
+            else if (SL <= 0.0f && SZL >= 0.0f) region = 2;
+            else if (SL > 0.0f) region = 1;
+            else region = 0;
         }
-        if (SR < 0.0f) region = 6;
-        else if (SM <= 0.0f && SR >= 0.0f) region = 5;
-        else if (SL <= 0.0f && SM >= 0.0f) region = 2;
-        else if (SL > 0.0f) region = 1;
-        else region = 0;
-    } else {             // HLLD (:1598-1814)
-        const F2 rsupt = rsu * mk(pt.y, pt.x);           // (suL r1 ptR, suR r2 ptL)
-        ptz = ((rsupt.y - rsupt.x) + r.x * r.y * su.y * su.x * (u.y - u.x)) * idd;
-        const float bn2 = bn * bn;
-        const F2 tt = rsu * sm - splat(bn2);             // r su (S - SM) - bn^2
-        const F2 itt = rcp2(tt);
-        const bool degL = fabsf(tt.x) <= (float)kTtEps, degR = fabsf(tt.y) <= (float)kTtEps;
-        F2 tv = (splat(SM) - u) * itt;
-        F2 tb = fma2(rsu, su, splat(-bn2)) * itt;        // (r su^2 - bn^2) / tt
-        if (degL) tv.x = tb.x = 0.0f;
-        if (degR) tv.y = tb.y = 0.0f;
-        const F2 nbn = splat(-bn);
-        vz2 = fma2(nbn, by * tv, v);
-        vz3 = fma2(nbn, bz * tv, w);
-        bz2 = by * tb;
-        bz3 = bz * tb;
-        const F2 isq = rsqrt2(rz);
-        rzs = rz * isq;
-        const float abn = fabsf(bn);
-        if (abn > (float)kEpsB) {
-            ibn = true;
-            sbn = bn > 0.0f ? 1.0f : -1.0f;
-            SZL = SM - abn * isq.x;
-            SZR = SM + abn * isq.y;
-        }
-        if (SR < 0.0f) region = 6;
-        else if (SZR <= 0.0f && SR >= 0.0f) region = 5;
-        else if (ibn && SM <= 0.0f && SZR >= 0.0f) region = 4;
-        else if (ibn && SZL <= 0.0f && SM >= 0.0f) region = 3;
-        else if (SL <= 0.0f && SZL >= 0.0f) region = 2;
-        else if (SL > 0.0f) region = 1;
-        else region = 0;
     }
     int flag = region == 0 ? kFlagWave : 0;
     const bool right = region >= 4;
     const bool use1 = (region >= 2 && region <= 5);
     const bool use2 = (region == 3 || region == 4);
-    float vzz2 = 0.0f, vzz3 = 0.0f, bzz2 = 0.0f, bzz3 = 0.0f;
-    if (NSTATE == 3 && use2) {   // double-star state (:1658-1718)
-        const float irzss = sb_rcp(rzs.y + rzs.x);
-        const float rzps = rzs.y * rzs.x;
-        vzz2 = ((rzs.x * vz2.x + rzs.y * vz2.y) + sbn * (bz2.y - bz2.x)) * irzss;
-        vzz3 = ((rzs.x * vz3.x + rzs.y * vz3.y) + sbn * (bz3.y - bz3.x)) * irzss;
-        bzz2 = ((rzs.x * bz2.y + rzs.y * bz2.x) + sbn * rzps * (vz2.y - vz2.x)) * irzss;
-        bzz3 = ((rzs.x * bz3.y + rzs.y * bz3.x) + sbn * rzps * (vz3.y - vz3.x)) * irzss;
-    }
 
-    // the selected side: energy, physical flux, conserved vector, star energy (:1368-1404,
-    // :1541-1544 / :1650-1656, :1710-1718)
+    // the selected side: energy, physical flux, conserved vector (:1368-1404)
     const float rr = pick(r, right), uu = pick(u, right), vv = pick(v, right), ww = pick(w, right);
     const float pp = pick(p, right), bxs = pick(bx, right), bys = pick(by, right), bzs = pick(bz, right);
-    const float pts = pick(pt, right), b2s = pick(b2, right), sums = pick(sum, right), isms = pick(ism, right);
-    const float rzz = pick(rz, right), S1 = right ? SR : SL, S2 = right ? SZR : SZL;
-    const float v2s = pick(vz2, right), v3s = pick(vz3, right), b2z = pick(bz2, right), b3z = pick(bz3, right);
+    const float pts = pick(pt, right), b2s = pick(b2, right);
     const float e = (pp * (float)kInvG1 + rr * (half * ((uu * uu + vv * vv) + ww * ww))) + half * b2s;
     const float sbv = (uu * bxs + vv * bys) + ww * bzs;
     const float m = rr * uu;
-    const float sbvS = NSTATE == 2 ? sbvz : (bn * SM + b2z * v2s) + b3z * v3s;
-    const float ez = e * sums + (((ptz * SM - pts * uu) + bn * (sbv - sbvS)) * isms);
-    float ezz = ez;
-    if (NSTATE == 3 && use2) {
-        const float sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
-        ezz = right ? ez + pick(rzs, true) * sbn * (sbvS - sbzz) : ez - pick(rzs, false) * sbn * (sbvS - sbzz);
-    }
     // the two tangential components of each vector, and the flux assembly, as f32x2 pairs
     const F2 vw = mk(vv, ww), bt = mk(bys, bzs);
     const F2 fs23 = fma2(splat(m), vw, splat(-bxs) * bt);   // m v - bx by, m w - bx bz
     const F2 fs67 = fma2(splat(uu), bt, splat(-bxs) * vw);  // u by - v bx, u bz - w bx
-    const F2 us23 = splat(rr) * vw, uz23 = splat(rzz) * mk(v2s, v3s), uzz23 = splat(rzz) * mk(vzz2, vzz3);
-    const F2 Fs[4] = {mk(m, (m * uu + pts) - bxs * bxs), fs23, mk((e + pts) * uu - bxs * sbv, 0.0f), fs67};
-    const F2 Us[4] = {mk(rr, m), us23, mk(e, bxs), bt};
-    const F2 UZs[4] = {mk(rzz, rzz * SM), uz23, mk(ez, bn), mk(b2z, b3z)};
-    const F2 UZZs[4] = {mk(rzz, rzz * SM), uzz23, mk(ezz, bn), mk(bzz2, bzz3)};
+    const F2 us23 = splat(rr) * vw;
+    F2 Fo[4] = {mk(m, (m * uu + pts) - bxs * bxs), fs23, mk((e + pts) * uu - bxs * sbv, 0.0f), fs67};
+    if (use1) {
+        // the star state of the selected side and its energy (:1541-1544 / :1650-1656), the
+        // double-star state (:1658-1718)
+        float vzz2 = 0.0f, vzz3 = 0.0f, bzz2 = 0.0f, bzz3 = 0.0f;
+        if (NSTATE == 3 && use2) {
+            const float irzss = sb_rcp(rzs.y + rzs.x);
+            const float rzps = rzs.y * rzs.x;
+            vzz2 = ((rzs.x * vz2.x + rzs.y * vz2.y) + sbn * (bz2.y - bz2.x)) * irzss;
+            vzz3 = ((rzs.x * vz3.x + rzs.y * vz3.y) + sbn * (bz3.y - bz3.x)) * irzss;
+            bzz2 = ((rzs.x * bz2.y + rzs.y * bz2.x) + sbn * rzps * (vz2.y - vz2.x)) * irzss;
+            bzz3 = ((rzs.x * bz3.y + rzs.y * bz3.x) + sbn * rzps * (vz3.y - vz3.x)) * irzss;
+        }
+        const float sums = pick(sum, right), isms = pick(ism, right);
+        const float rzz = pick(rz, right), S1 = right ? SR : SL, S2 = right ? SZR : SZL;
+        const float v2s = pick(vz2, right), v3s = pick(vz3, right), b2z = pick(bz2, right), b3z = pick(bz3, right);
+        const float sbvS = NSTATE == 2 ? sbvz : (bn * SM + b2z * v2s) + b3z * v3s;
+        const float ez = e * sums + (((ptz * SM - pts * uu) + bn * (sbv - sbvS)) * isms);
+        float ezz = ez;
+        if (NSTATE == 3 && use2) {
+            const float sbzz = (bn * SM + bzz2 * vzz2) + bzz3 * vzz3;
+            ezz = right ? ez + pick(rzs, true) * sbn * (sbvS - sbzz) : ez - pick(rzs, false) * sbn * (sbvS - sbzz);
+        }
+        const F2 uz23 = splat(rzz) * mk(v2s, v3s), uzz23 = splat(rzz) * mk(vzz2, vzz3);
+        const F2 Us[4] = {mk(rr, m), us23, mk(e, bxs), bt};
+        const F2 UZs[4] = {mk(rzz, rzz * SM), uz23, mk(ez, bn), mk(b2z, b3z)};
+        const F2 UZZs[4] = {mk(rzz, rzz * SM), uzz23, mk(ezz, bn), mk(bzz2, bzz3)};
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        F2 f = Fs[k];
-        if (use2) f = fma2(splat(S2), UZZs[k] - UZs[k], f);
-        if (use1) f = fma2(splat(S1), UZs[k] - Us[k], f);
-        F[2 * k] = f.x;
-        F[2 * k + 1] = f.y;
-    }
-    if (use1) {   // positivity of the selected star state (rho* > 0, p* = pt* - |b*|^2/2 > 0)
+        for (int k = 0; k < 4; k++) {
+            F2 f = Fo[k];
+            if (use2) f = fma2(splat(S2), UZZs[k] - UZs[k], f);
+            Fo[k] = fma2(splat(S1), UZs[k] - Us[k], f);
+        }
+        // positivity of the selected star state (rho* > 0, p* = pt* - |b*|^2/2 > 0)
         const float w6 = use2 ? bzz2 : b2z, w7 = use2 ? bzz3 : b3z;
         if (!(rzz > 0.0f) || !(ptz - half * ((bn * bn + w6 * w6) + w7 * w7) > 0.0f)) flag |= kFlagStar;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        F[2 * k] = Fo[k].x;
+        F[2 * k + 1] = Fo[k].y;
     }
     // normal-field flux (:1570-1581 / :1828-1839) and B fluxes back to stored units (:1846)
     const float spi4 = (float)kSpi4;
