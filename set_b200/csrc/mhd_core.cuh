@@ -668,22 +668,28 @@ struct DeltaIn {   // FP32 side values (b = B / sqrt(4 pi)), their jumps, energi
     float du, dv, dw, dbx, dby, dbz, dpt;
 };
 
+// The fast magnetosonic speeds of the two sides (as riemann()), from d's r, p, bx and |b|^2.
+SB_HD void delta_fast_speeds(const DeltaIn& d, float& cfL, float& cfR) {
+    typedef float f;
+    const f ga = (f)kGamma, half = 0.5f;
+    const f ir1 = sb_rcp(d.r1), ir2 = sb_rcp(d.r2);
+    const f c2L = ga * d.p1 * ir1, c2R = ga * d.p2 * ir2;
+    const f sL = c2L + d.b2L * ir1, sR = c2R + d.b2R * ir2;
+    cfL = sb_sqrt(half * (sL + sb_sqrt(sb_pos(sL * sL - 4.0f * c2L * (d.bx1 * d.bx1 * ir1)))));
+    cfR = sb_sqrt(half * (sR + sb_sqrt(sb_pos(sR * sR - 4.0f * c2R * (d.bx2 * d.bx2 * ir2)))));
+}
+
 // Returns kFlagWave / kFlagStar like riemann() and sets `right` (the selected side) and c[8]:
 // the flux minus the physical flux of the selected side, c[5] the whole normal-field flux.
+// cfL, cfR: delta_fast_speeds of d.
 template <int NSTATE>
-SB_HD int delta_core(const DeltaIn& d, float* c, bool& right, float& SLo, float& SRo, float& SMo) {
+SB_HD int delta_core(const DeltaIn& d, float cfL, float cfR, float* c, bool& right, float& SLo, float& SRo,
+                     float& SMo) {
     typedef float f;
     const f fr1 = d.r1, fu1 = d.u1, fv1 = d.v1, fw1 = d.w1, fr2 = d.r2, fu2 = d.u2, fv2 = d.v2, fw2 = d.w2;
     const f fbx1 = d.bx1, fby1 = d.by1, fbz1 = d.bz1, fbx2 = d.bx2, fby2 = d.by2, fbz2 = d.bz2;
     const f du = d.du, dv = d.dv, dw = d.dw, dbx = d.dbx, dby = d.dby, dbz = d.dbz, dpt = d.dpt;
-
-    // fast speeds (as riemann())
-    const f ga = (f)kGamma, half = 0.5f;
-    const f ir1 = sb_rcp(fr1), ir2 = sb_rcp(fr2);
-    const f c2L = ga * d.p1 * ir1, c2R = ga * d.p2 * ir2;
-    const f sL = c2L + d.b2L * ir1, sR = c2R + d.b2R * ir2;
-    const f cfL = sb_sqrt(half * (sL + sb_sqrt(sb_pos(sL * sL - 4.0f * c2L * (fbx1 * fbx1 * ir1)))));
-    const f cfR = sb_sqrt(half * (sR + sb_sqrt(sb_pos(sR * sR - 4.0f * c2R * (fbx2 * fbx2 * ir2)))));
+    const f half = 0.5f;
 
     // speeds relative to each side: SL - u1 = min(-cfL, du - cfR), SR - u2 = max(cfL - du, cfR)
     const f suL = sb_min(-cfL, du - cfR);
@@ -836,19 +842,45 @@ SB_HD int riemann_delta(const D* q1, const D* q2, D* F, float& SLo, float& SRo, 
     const D b2R = (bx2 * bx2 + by2 * by2) + bz2 * bz2;
     const D ptL = p1 + D(0.5) * b2L, ptR = p2 + D(0.5) * b2R;
     if (NSTATE == 2 && (b2L != D(0) || b2R != D(0))) return kFlagStar;
-    const D e1 = (p1 * D(kInvG1) + r1 * (D(0.5) * ((u1 * u1 + v1 * v1) + w1 * w1))) + D(0.5) * b2L;
-    const D e2 = (p2 * D(kInvG1) + r2 * (D(0.5) * ((u2 * u2 + v2 * v2) + w2 * w2))) + D(0.5) * b2R;
+    // First the values the wave speeds and SM need.  SR < 0 selects FR (the last match of the
+    // region chain) whatever the star states are, and FR's flux is the right side's physical flux
+    // with c = 0 but the normal-field term, so the remaining conversions and the star states are
+    // made only where some other region may be selected.
     DeltaIn d;
-    d.r1 = (f)r1; d.u1 = (f)u1; d.v1 = (f)v1; d.w1 = (f)w1; d.p1 = (f)p1;
-    d.bx1 = (f)bx1; d.by1 = (f)by1; d.bz1 = (f)bz1; d.b2L = (f)b2L; d.e1 = (f)e1; d.ptL = (f)ptL;
-    d.r2 = (f)r2; d.u2 = (f)u2; d.v2 = (f)v2; d.w2 = (f)w2; d.p2 = (f)p2;
-    d.bx2 = (f)bx2; d.by2 = (f)by2; d.bz2 = (f)bz2; d.b2R = (f)b2R; d.e2 = (f)e2;
-    d.du = (f)(u2 - u1); d.dv = (f)(v2 - v1); d.dw = (f)(w2 - w1);
-    d.dbx = (f)(bx2 - bx1); d.dby = (f)(by2 - by1); d.dbz = (f)(bz2 - bz1);
+    d.r1 = (f)r1; d.u1 = (f)u1; d.p1 = (f)p1; d.bx1 = (f)bx1; d.b2L = (f)b2L;
+    d.r2 = (f)r2; d.u2 = (f)u2; d.p2 = (f)p2; d.bx2 = (f)bx2; d.b2R = (f)b2R;
+    d.du = (f)(u2 - u1);
+    d.dbx = (f)(bx2 - bx1);
     d.dpt = (f)(ptR - ptL);
+    float cfL, cfR;
+    delta_fast_speeds(d, cfL, cfR);
     float c[8];
-    bool right;
-    const int flag = delta_core<NSTATE>(d, c, right, SLo, SRo, SMo);
+    bool right = true;
+    int flag;
+    D e1 = D(0), e2 = D(0);
+    const f suR = sb_max(cfL - d.du, cfR);
+    const f SR = d.u2 + suR;
+    if (SR < 0.0f) {
+        const f suL = sb_min(-cfL, d.du - cfR);
+        const f SL = d.u1 + suL;
+        const f iden = sb_rcp(suR * d.r2 - suL * d.r1);
+        SLo = SL;
+        SRo = SR;
+        SMo = d.u1 + (suR * d.r2 * d.du - d.dpt) * iden;
+#pragma unroll
+        for (int k = 0; k < 8; k++) c[k] = 0.0f;
+        c[5] = NSTATE == 3 ? -sb_max(sb_abs(SL), sb_abs(SR)) * d.dbx : 0.0f;
+        flag = (!(sb_abs(SL) < 3.0e38f) || !(sb_abs(SR) < 3.0e38f)) ? kFlagStar : 0;
+        e2 = (p2 * D(kInvG1) + r2 * (D(0.5) * ((u2 * u2 + v2 * v2) + w2 * w2))) + D(0.5) * b2R;
+    } else {
+        e1 = (p1 * D(kInvG1) + r1 * (D(0.5) * ((u1 * u1 + v1 * v1) + w1 * w1))) + D(0.5) * b2L;
+        e2 = (p2 * D(kInvG1) + r2 * (D(0.5) * ((u2 * u2 + v2 * v2) + w2 * w2))) + D(0.5) * b2R;
+        d.v1 = (f)v1; d.w1 = (f)w1; d.by1 = (f)by1; d.bz1 = (f)bz1; d.e1 = (f)e1; d.ptL = (f)ptL;
+        d.v2 = (f)v2; d.w2 = (f)w2; d.by2 = (f)by2; d.bz2 = (f)bz2; d.e2 = (f)e2;
+        d.dv = (f)(v2 - v1); d.dw = (f)(w2 - w1);
+        d.dby = (f)(by2 - by1); d.dbz = (f)(bz2 - bz1);
+        flag = delta_core<NSTATE>(d, cfL, cfR, c, right, SLo, SRo, SMo);
+    }
     // physical flux of the selected side
     const D r = right ? r2 : r1, u = right ? u2 : u1, v = right ? v2 : v1, w = right ? w2 : w1;
     const D bx = right ? bx2 : bx1, by = right ? by2 : by1, bz = right ? bz2 : bz1;
