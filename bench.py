@@ -42,12 +42,13 @@ BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
 BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
 BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
 # DRAM bytes (read + write) per cell of one plain stage-2 launch, from an ncu capture of that
-# kernel at 160^3 (1.0407 TB/s x 743.4 us = 773.6 MB / 4.096 M cells); traffic grows with the
-# cell count, so the full-size launch's traffic is this figure times its cells.
-TRAFFIC_STAGE2_PER_CELL = 773.6e6 / 160 ** 3
+# kernel at 160^3 (dram__bytes_read.sum 548.7 MB + dram__bytes_write.sum 225.4 MB over 4.096 M
+# cells); traffic grows with the cell count, so the full-size launch's traffic is this figure
+# times its cells.
+TRAFFIC_STAGE2_PER_CELL = 774.1e6 / 160 ** 3
 # FP64 pipe thread instructions (DFMA + DMUL + DADD + DSETP) per cell of the same launch, from
-# the same capture's opcode counts (163.73 M warp instructions x 30.88 threads / 4.096 M cells).
-FP64_OPS_STAGE2_PER_CELL = 1234
+# the same capture's opcode counts (138.49 M warp instructions x 30.95 threads / 4.096 M cells).
+FP64_OPS_STAGE2_PER_CELL = 1046
 
 
 def peaks():
@@ -568,7 +569,8 @@ def run_ours(args, world, rank, local):
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
                          "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
                          "limiter": "the FP64 pipe and instruction issue, not DRAM: at 160^3 ncu shows DRAM "
-                                    "traffic 0.98x algorithmic, FP64 pipe 42-44 %, issue 47-48 % at 12 warps/SM",
+                                    "traffic 0.98x algorithmic, FP64 pipe 39-40 %, issue 46-47 % at 12 warps/SM, "
+                                    "top stall FP64 dependency latency",
                          "fp64_pipe": {"ops_per_cell": FP64_OPS_STAGE2_PER_CELL, "achieved_tops": fp64_ach,
                                        "peak_tops": fp64_peak, "frac": fp64_ach / fp64_peak,
                                        "source": "DFMA + DMUL + DADD + DSETP thread instructions per cell of the "
