@@ -65,11 +65,26 @@ class Server:
         self.close()
 
 
+def _warm(requests, precision: int, check_every: int):
+    """One untimed short solve (one check interval) per distinct solver option set of the stream,
+    so a timed run does not pay the kernels' first-use loading."""
+    seen = set()
+    for rq in requests:
+        o = rq.inst.opts
+        key = (o.n_state, o.n_disc, o.order, o.scheme)
+        if key not in seen:
+            seen.add(key)
+            solve_alone(rq.inst, precision, rq.steady_tol, check_every, check_every)
+
+
 def run_stream(requests, max_slots: int = 256, precision: int = 1, hbm_budget: int = 150 * 10 ** 9,
-               check_every: int = 50, keep=()):
+               check_every: int = 50, keep=(), warm: bool = True):
     """Submits each request at its arrival time (seconds from the start) and waits for all.
-    Returns latencies (done - submit, server clock), solves/s over the stream, and results."""
+    Returns latencies (done - submit, server clock), solves/s over the stream, and results.
+    `warm`: the kernels are loaded by untimed short solves first (as for run_sequential)."""
     keep = set(keep)
+    if warm:
+        _warm(requests, precision, check_every)
     with Server(max_slots, precision, hbm_budget, check_every) as srv:
         t0 = time.perf_counter()
         ids = []
@@ -129,8 +144,11 @@ def solve_alone(inst, precision: int = 0, steady_tol: float = 1e-5, max_steps: i
     return {"steps": steps, "converged": conv, "last_change": last, "U": U, "diag": d, "status": status}
 
 
-def run_sequential(requests, precision: int = 0, check_every: int = 50):
-    """The same requests processed one at a time, back to back (arrival gaps ignored)."""
+def run_sequential(requests, precision: int = 0, check_every: int = 50, warm: bool = True):
+    """The same requests processed one at a time, back to back (arrival gaps ignored).  `warm`:
+    untimed short solves first (_warm)."""
+    if warm:
+        _warm(requests, precision, check_every)
     t0 = time.perf_counter()
     out = [solve_alone(rq.inst, precision, rq.steady_tol, rq.max_steps, check_every) for rq in requests]
     secs = time.perf_counter() - t0
