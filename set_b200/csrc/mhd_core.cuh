@@ -829,8 +829,8 @@ SB_HD int delta_core(const DeltaIn& d, float cfL, float cfR, float* c, bool& rig
 // Delta form on face states held in type D (FP64 in the delta form): side values rounded to
 // FP32, jumps formed in D then rounded, and the physical flux of the selected side in D.
 // kFlagStar also when NSTATE 2 sees a magnetic field (the delta form covers hydro HLLC only) --
-// the caller then recomputes the face in FP64.
-template <int NSTATE, typename D = double>
+// the caller then recomputes the face in FP64.  LAZY: FR faces skip the star states (below).
+template <int NSTATE, typename D = double, bool LAZY = true>
 SB_HD int riemann_delta(const D* q1, const D* q2, D* F, float& SLo, float& SRo, float& SMo) {
     typedef float f;
     const D ispi4 = D(kInvSpi4);
@@ -860,7 +860,7 @@ SB_HD int riemann_delta(const D* q1, const D* q2, D* F, float& SLo, float& SRo, 
     D e1 = D(0), e2 = D(0);
     const f suR = sb_max(cfL - d.du, cfR);
     const f SR = d.u2 + suR;
-    if (SR < 0.0f) {
+    if (LAZY && SR < 0.0f) {
         const f suL = sb_min(-cfL, d.du - cfR);
         const f SL = d.u1 + suL;
         const f iden = sb_rcp(suR * d.r2 - suL * d.r1);
