@@ -65,7 +65,7 @@ class Server:
         self.close()
 
 
-def _warm(requests, precision: int, check_every: int):
+def warm_kernels(requests, precision: int, check_every: int = 50):
     """One untimed short solve (one check interval) per distinct solver option set of the stream,
     so a timed run does not pay the kernels' first-use loading."""
     seen = set()
@@ -84,7 +84,7 @@ def run_stream(requests, max_slots: int = 256, precision: int = 1, hbm_budget: i
     `warm`: the kernels are loaded by untimed short solves first (as for run_sequential)."""
     keep = set(keep)
     if warm:
-        _warm(requests, precision, check_every)
+        warm_kernels(requests, precision, check_every)
     with Server(max_slots, precision, hbm_budget, check_every) as srv:
         t0 = time.perf_counter()
         ids = []
@@ -146,9 +146,9 @@ def solve_alone(inst, precision: int = 0, steady_tol: float = 1e-5, max_steps: i
 
 def run_sequential(requests, precision: int = 0, check_every: int = 50, warm: bool = True):
     """The same requests processed one at a time, back to back (arrival gaps ignored).  `warm`:
-    untimed short solves first (_warm)."""
+    untimed short solves first (warm_kernels)."""
     if warm:
-        _warm(requests, precision, check_every)
+        warm_kernels(requests, precision, check_every)
     t0 = time.perf_counter()
     out = [solve_alone(rq.inst, precision, rq.steady_tol, rq.max_steps, check_every) for rq in requests]
     secs = time.perf_counter() - t0
