@@ -99,11 +99,13 @@ SB_HD float sb_rsqrt(float x) {
 // (tests/test_gpu_special.py checks 2^20 inputs over 1e-300..1e300).  At 0 and +-inf 1/x and
 // 1/sqrt(x) give NaN; at subnormals 1/x gives NaN and 1/sqrt(x) +inf (sqrt(0) = 0).  Every
 // argument the flux passes them is a positive density, a sum of squares under sb_pos, or a
-// wave-speed difference that a valid state keeps away from zero (SR - SL >= cfL + cfR > 0; the star denominators tt are screened against 1e-9 before the reciprocal); a
-// state that is already invalid (rho <= 0) is reported by the cell update's counters either way.
-// Three (1/x), five (1/sqrt(x)) and six (sqrt(x)) FP64 operations after the seed: fewer than the
-// correctly rounded library forms, on the pipe that bounds the plain form; the state conversions,
-// the mixed form and the out-of-line FP64 recomputes keep the library forms.  On the host all
+// wave-speed difference that a valid state keeps away from zero (SR - SL >= cfL + cfR > 0; the
+// star denominators tt are screened against 1e-9 before the reciprocal); a state that is already
+// invalid (rho <= 0) is reported by the cell update's counters either way.  Three (1/x), five
+// (1/sqrt(x)) and six (sqrt(x)) FP64 operations after the seed: fewer than the correctly rounded
+// library forms, on the pipe that bounds the plain form.  The guarded primitive recovery's cheap
+// path uses rs_rcp too; the exact recovery, the mixed form and the out-of-line FP64 recomputes
+// keep the library forms.  On the host all
 // three are the IEEE operations.
 SB_HD double rs_rcp(double x) {
 #if defined(__CUDA_ARCH__)
@@ -290,6 +292,37 @@ SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
     q[6] = SB ? by : U[6];
     q[7] = SB ? bz : U[7];
 }
+// The exact recovery where it matters, at about half its cost elsewhere: velocities and b from a
+// one-ulp reciprocal (rs_rcp) and multiplies, ke, me, p with contraction.  Each velocity and b is
+// then within 4 ulps of the exact quotient and p within about 12 (ke + me) / p + 2 E / p ulps of
+// the exact recovery's; where the kinetic and magnetic energies exceed 64 p (the hypersonic
+// outflow of the source, where one ulp of a velocity moves p by ~1e-12), or p is not positive or
+// not finite, the exact recovery is run instead, so the state differs from the oracle's by at
+// most ~1e-13 relative in p and 4 ulps elsewhere.  SB as prim_from_cons.
+template <bool SB = false>
+SB_HD void prim_from_cons_guarded(const double* U, double* q) {
+    const double rho = U[0];
+    const double ir = rs_rcp(rho);
+    const double u = U[1] * ir, v = U[2] * ir, w = U[3] * ir;
+    const double bx = U[5] * kInvSpi4, by = U[6] * kInvSpi4, bz = U[7] * kInvSpi4;
+    const double ke = 0.5 * rho * ((u * u + v * v) + w * w);
+    const double me = 0.5 * ((bx * bx + by * by) + bz * bz);
+    const double p = ((U[4] - ke) - me) * kG1;
+    if (!(ke + me <= 64.0 * p)) {
+        double ke2, me2;
+        prim_from_cons<true, SB>(U, q, ke2, me2);
+        return;
+    }
+    q[0] = rho;
+    q[1] = u;
+    q[2] = v;
+    q[3] = w;
+    q[4] = p;
+    q[5] = SB ? bx : U[5];
+    q[6] = SB ? by : U[6];
+    q[7] = SB ? bz : U[7];
+}
+
 // Total energy at the pressure floor, (p_floor/(gamma-1) + ke) + me: the oracle's cons_from_prim
 // of the floored state (cuf_solvers.cuf:777-779), with ke, me from prim_from_cons<true>.
 constexpr double kPFloorE = kPFloor / kG1;

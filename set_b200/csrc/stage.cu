@@ -75,8 +75,12 @@ __device__ __forceinline__ void fetch_prim64(const StageArgs& A, int i, int j, i
     double U[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) U[v] = __ldg(A.Uin + v * g.vs + off);
-    double ke, me;
-    prim_from_cons<EXACT, SB>(U, q, ke, me);
+    if constexpr (EXACT) {
+        prim_from_cons_guarded<SB>(U, q);
+    } else {
+        double ke, me;
+        prim_from_cons<false, SB>(U, q, ke, me);
+    }
 }
 
 // Loads plane kk (with halo) of the tile starting at (i0, j0) as primitives into `dst`.
@@ -168,8 +172,12 @@ __device__ __forceinline__ void convert_plane(const StageArgs& A, const double* 
             double U[8];
 #pragma unroll
             for (int v = 0; v < 8; v++) U[v] = src[v * PLANE];
-            double ke, me;
-            prim_from_cons<P != 1, P == 0>(U, q, ke, me);
+            if constexpr (P == 1) {
+                double ke, me;
+                prim_from_cons<false, false>(U, q, ke, me);
+            } else {
+                prim_from_cons_guarded<P == 0>(U, q);
+            }
         }
 #pragma unroll
         for (int v = 0; v < 8; v++) dst[v * PLANE + c] = (RT)q[v];

@@ -1,7 +1,7 @@
 // Test-only kernels: the region-first (LAZY) and branch-free (eager) instantiations of the
 // Riemann solvers of set_b200/csrc/mhd_core.cuh side by side on the same face states, and the
-// quick pressure-positivity test next to the exact primitive recovery.  Built by
-// tests/test_gpu_solver_paths.py with nvcc for sm_100a into a temporary library.
+// quick pressure-positivity test and the guarded primitive recovery next to the exact recovery.
+// Built by tests/test_gpu_solver_paths.py with nvcc for sm_100a into a temporary library.
 #include <cuda_runtime.h>
 #include "mhd_core.cuh"
 
@@ -64,6 +64,15 @@ __global__ void ptest_kernel(const double* U, int* out, long long n) {
     prim_from_cons<true>(U + 8 * i, q, ke, me);
     out[2 * i] = pressure_surely_positive(U + 8 * i) ? 1 : 0;
     out[2 * i + 1] = q[4] > 0.0 ? 1 : 0;
+}
+
+// out[16 i .. 16 i + 7] = prim_from_cons_guarded(U), out[16 i + 8 ..] = prim_from_cons<true>(U)
+__global__ void guarded_kernel(const double* U, double* out, long long n) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double ke, me;
+    prim_from_cons_guarded(U + 8 * i, out + 16 * i);
+    prim_from_cons<true>(U + 8 * i, out + 16 * i + 8, ke, me);
 }
 
 struct DevBuf {
@@ -132,5 +141,15 @@ extern "C" int pressure_test(const double* U, long long n, int* out) {
     ptest_kernel<<<(unsigned)((n + 255) / 256), 256>>>((const double*)u.p, (int*)o.p, n);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return 3;
     if (cudaMemcpy(out, o.p, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost)) return 4;
+    return 0;
+}
+
+extern "C" int guarded_recovery(const double* U, long long n, double* out) {
+    DevBuf u, o;
+    if (cudaMalloc(&u.p, sizeof(double) * 8 * n) || cudaMalloc(&o.p, sizeof(double) * 16 * n)) return 1;
+    if (cudaMemcpy(u.p, U, sizeof(double) * 8 * n, cudaMemcpyHostToDevice)) return 2;
+    guarded_kernel<<<(unsigned)((n + 255) / 256), 256>>>((const double*)u.p, (double*)o.p, n);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return 3;
+    if (cudaMemcpy(out, o.p, sizeof(double) * 16 * n, cudaMemcpyDeviceToHost)) return 4;
     return 0;
 }

@@ -10,7 +10,8 @@ and the two forms place the same expressions in different blocks.  Measured on a
 fluxes within ~2e-14 of the face's largest flux component (~98 % of faces bit for bit), HLLC
 within ~2e-13 (~1/3 bit for bit); the delta form to its FP32 corrections' rounding.  The
 pressure floor's quick test (pressure_surely_positive) must never clear a state whose exact
-recovery gives p <= 0.
+recovery gives p <= 0, and the guarded primitive recovery (prim_from_cons_guarded) must be the
+exact one where it matters and within stated bounds elsewhere.
 
 tests/csrc/solver_paths.cu wraps the instantiations in kernels; this test compiles it with nvcc
 for sm_100a into a temporary library.
@@ -47,6 +48,8 @@ def sp_lib(tmp_path_factory):
     lib.delta_pair.argtypes = [dp, dp, C.c_longlong, C.c_int, dp, dp]
     lib.pressure_test.restype = C.c_int
     lib.pressure_test.argtypes = [dp, C.c_longlong, C.POINTER(C.c_int)]
+    lib.guarded_recovery.restype = C.c_int
+    lib.guarded_recovery.argtypes = [dp, C.c_longlong, dp]
     return lib
 
 
@@ -162,3 +165,34 @@ def test_quick_pressure_test_never_clears_a_floored_state(sp_lib):
     # the quick test clears nearly every state away from the floor; the edge set holds floored ones
     assert quick[~edge].mean() > 0.999
     assert (~exact[edge]).sum() > 1000
+
+
+def test_guarded_recovery_is_the_exact_one_where_it_matters(sp_lib):
+    """prim_from_cons_guarded: the exact recovery bit for bit wherever ke + me > 64 p (the
+    hypersonic source outflow); elsewhere each velocity is the product with a one-ulp reciprocal,
+    within 4 ulps of the correctly rounded quotient, and p within 1e-13 relative (about
+    12 (ke + me) / p + 2 E / p ulps, at most ~8.5e-14 under the guard)."""
+    rng = np.random.default_rng(9)
+    n = 1 << 20
+    rho = 10.0 ** rng.uniform(-3, 2, n)
+    vel = rng.uniform(-1, 1, (n, 3)) * (10.0 ** rng.uniform(-2, 2, n))[:, None]
+    B = rng.uniform(-3, 3, (n, 3)) * (rng.random(n) < 0.8)[:, None]
+    p = 10.0 ** rng.uniform(-4, 1, n)
+    U = np.empty((n, 8))
+    U[:, 0] = rho
+    U[:, 1:4] = rho[:, None] * vel
+    U[:, 5:8] = B
+    ke = 0.5 * rho * (vel ** 2).sum(1)
+    me = 0.5 * (B ** 2).sum(1) / (4.0 * np.pi)
+    U[:, 4] = p * 1.5 + ke + me
+    out = np.zeros((n, 16))
+    assert sp_lib.guarded_recovery(_ptr(U), n, _ptr(out)) == 0
+    g, x = out[:, :8], out[:, 8:]
+    hyper = ~(ke + me <= 64.0 * x[:, 4])
+    assert 0.05 < hyper.mean() < 0.95, hyper.mean()
+    assert _bits_equal(g[hyper], x[hyper])
+    cheap = ~hyper
+    assert np.array_equal(g[cheap][:, [0, 5, 6, 7]], x[cheap][:, [0, 5, 6, 7]])
+    gu, xu = g[cheap][:, 1:4], x[cheap][:, 1:4]
+    assert (np.abs(gu.view(np.int64) - xu.view(np.int64))[xu != 0] <= 4).all()
+    assert np.max(np.abs(g[cheap][:, 4] - x[cheap][:, 4]) / x[cheap][:, 4]) <= 1e-13
