@@ -42,13 +42,13 @@ BYTES_STAGE1 = 128   # read U^n (8 x f64), write U* (8 x f64)
 BYTES_STAGE2 = 192   # read U*, U^n, write U^n+1
 BYTES_STEP = BYTES_STAGE1 + BYTES_STAGE2
 # DRAM bytes (read + write) per cell of one plain stage-2 launch, from an ncu capture of that
-# kernel at 160^3 (dram__bytes_read.sum 548.7 MB + dram__bytes_write.sum 225.4 MB over 4.096 M
+# kernel at 160^3 (dram__bytes_read.sum 549.3 MB + dram__bytes_write.sum 226.0 MB over 4.096 M
 # cells); traffic grows with the cell count, so the full-size launch's traffic is this figure
 # times its cells.
-TRAFFIC_STAGE2_PER_CELL = 774.1e6 / 160 ** 3
+TRAFFIC_STAGE2_PER_CELL = 775.4e6 / 160 ** 3
 # FP64 pipe thread instructions (DFMA + DMUL + DADD + DSETP) per cell of the same launch, from
-# the same capture's opcode counts (138.49 M warp instructions x 30.95 threads / 4.096 M cells).
-FP64_OPS_STAGE2_PER_CELL = 1046
+# the same capture's opcode counts (134.52 M warp instructions x 30.94 threads / 4.096 M cells).
+FP64_OPS_STAGE2_PER_CELL = 1016
 
 
 def peaks():
@@ -570,7 +570,7 @@ def run_ours(args, world, rank, local):
                          "stage1_ms": t1, "stage2_ms": t2, "step_achieved_gbs": ach_step,
                          "algorithmic_bytes_per_cell": {"stage1": BYTES_STAGE1, "stage2": BYTES_STAGE2},
                          "limiter": "the FP64 pipe and instruction issue, not DRAM: at 160^3 ncu shows DRAM "
-                                    "traffic 0.98x algorithmic, FP64 pipe 39-40 %, issue 46-47 % at 12 warps/SM, "
+                                    "traffic 0.99x algorithmic, FP64 pipe 38-40 %, issue 46-47 % at 12 warps/SM, "
                                     "top stall FP64 dependency latency",
                          "fp64_pipe": {"ops_per_cell": FP64_OPS_STAGE2_PER_CELL, "achieved_tops": fp64_ach,
                                        "peak_tops": fp64_peak, "frac": fp64_ach / fp64_peak,
