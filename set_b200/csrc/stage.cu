@@ -16,7 +16,9 @@
 //     (warp shuffle -> one atomicMin per CTA) are fused; the last CTA rolls the lagged-dt clock.
 //
 // P = 0, plain form: everything in FP64; the ring holds the field as b = B / sqrt(4 pi), the units
-//   the Riemann solver works in, and the primitives are recovered exactly as the oracle does.
+//   the Riemann solver works in, and the primitives are recovered exactly as the oracle does
+//   wherever the kinetic and magnetic energies exceed 64 p, within a few ulps elsewhere
+//   (prim_from_cons_guarded).
 // P = 1, mixed form: the ring holds FP32 primitives (recovered from the FP64 state in FP64),
 //   reconstruction and the Riemann solver run in FP32, fluxes are stored in FP32; a face whose
 //   selected FP32 state has rho <= 0 or p <= 0 (or a non-finite flux) is recomputed in FP64 from
