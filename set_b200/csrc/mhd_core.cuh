@@ -254,14 +254,14 @@ SB_HD double div_rn(double a, double b, double y) {
 // bit.  Pressure recovery cancels where the flow is hypersonic (the solar-wind source's outflow
 // runs at Mach ~77, where rho|v|^2/2 is ~3000 times p): there one ulp in a velocity moves p by
 // ~1e-12 relative, so a step computed from a differently rounded p differs from another correct
-// FP64 step by more than 1e-12 per cell.  !EXACT: one reciprocal and multiplies, with
-// contraction (the mixed form, which rounds the result to FP32).
+// FP64 step by more than 1e-12 per cell.  !EXACT: one one-ulp reciprocal (rs_rcp) and
+// multiplies, with contraction (the mixed form, which rounds the result to FP32).
 // SB: q[5..7] = b = B / sqrt(4 pi) (the field in the units the Riemann solver works in) instead of
 // the stored B.
 template <bool EXACT = true, bool SB = false>
 SB_HD void prim_from_cons(const double* U, double* q, double& ke, double& me) {
     const double rho = U[0];
-    const double ir = sb_rcp(rho);
+    const double ir = EXACT ? sb_rcp(rho) : rs_rcp(rho);   // Markstein's quotients need RN(1/rho)
     double u, v, w, bx, by, bz;
     if (EXACT) {
         u = div_rn(U[1], rho, ir);
